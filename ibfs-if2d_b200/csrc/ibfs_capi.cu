@@ -1,0 +1,955 @@
+// ibfs_capi.cu -- host runtime of the B200 IBFS advance behind include/ibfs_capi.h.
+//
+// A handle owns one or more cases (the batched form is the same code with
+// more items). At creation it builds, once, the whole step as a fixed list of
+// grouped launches (the "step program", mirroring advance, operators.f90:62-188)
+// and captures it into a CUDA graph that every step replays. Host work per
+// step is one graph launch (plus output copies when asked for).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/ibfs_capi.h"
+#include "ibfs_common.cuh"
+#include "ibfs_kernels.cuh"
+#include "ibfs_precision.cuh"
+
+namespace ibfs {
+
+static thread_local std::string t_error;
+
+int fail_cuda(cudaError_t e, const char* what) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "CUDA error %d (%s) at %s", (int)e, cudaGetErrorString(e), what);
+  t_error = buf;
+  return IBFS_ERR_CUDA;
+}
+
+static int fail(int code, const std::string& msg) {
+  t_error = msg;
+  return code;
+}
+
+// grid.f90:79: FLOOR(LOG(REAL(MIN(m,n)/2))/LOG(2.d0)) - 1 with single-precision LOG.
+static int nlevmax(int m, int n) {
+  int mn = std::min(m, n) / 2;
+  float lf = logf((float)mn);
+  return (int)std::floor((double)lf / std::log(2.0)) - 1;
+}
+
+// grid.f90:233-249.
+static double deltafnc(double r, double r0, double dr) {
+  double d = std::fabs(r - r0);
+  if (d <= 0.5 * dr) {
+    double t = (r - r0) / dr;
+    return (1.0 + std::sqrt(-3.0 * t * t + 1.0)) / (3.0 * dr);
+  } else if (d <= 1.5 * dr) {
+    double a = std::fabs((r - r0) / dr);
+    double u = 1.0 - a;
+    return (5.0 - 3.0 * a - std::sqrt(-3.0 * u * u + 1.0)) / (6.0 * dr);
+  }
+  return 0.0;
+}
+
+struct HostCase {
+  ibfs_params_c p;
+  ibfs_options_c o;
+  int m, n, L, ns, nq, nb, nf, nring, nbody, bmin;
+  double delta, norm;
+  std::vector<double> xb, yb;
+  std::vector<int> bdyno;
+  std::vector<int> face_ptr, face_f, force_ptr, force_face;
+  std::vector<double> face_w, force_w, wsum;
+  bool have_chol = false;
+  int out_off = 0;
+  int itime = 0;
+  DevCase dc{};
+};
+
+}  // namespace ibfs
+
+using namespace ibfs;
+
+struct ibfs_handle {
+  std::vector<HostCase> cases;
+  std::vector<void*> allocs;
+  DevCase* d_cases = nullptr;
+  std::map<int, double*> sine;
+  std::map<int, double*> costab;
+  cudaStream_t st = nullptr;
+  std::vector<std::function<void()>> prog;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_ok = false;
+  int* d_status = nullptr;
+  int* d_itime = nullptr;
+  double* d_out = nullptr;
+  double* d_hist = nullptr;
+  int hist_steps = 0;
+  int out_stride = 0;
+  double* d_partial = nullptr;
+  std::string err;
+  float last_ms = 0.f;
+  int tile_cfg = -1;
+  int precision = 0;
+  PrecisionPlan* prec = nullptr;
+  int max_ns = 0, max_nq = 0, max_nf = 0, max_ring = 0, max_L = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double* h_stage = nullptr;  // pinned staging for outputs / body velocities
+};
+
+namespace ibfs {
+
+template <class T>
+static T* dalloc(ibfs_handle* h, size_t count, bool zero = true) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) return nullptr;
+  if (zero) cudaMemset(p, 0, count * sizeof(T));
+  h->allocs.push_back(p);
+  return (T*)p;
+}
+
+template <class T>
+static T* dupload(ibfs_handle* h, const std::vector<T>& v) {
+  T* p = dalloc<T>(h, v.size(), false);
+  if (p && !v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return p;
+}
+
+// Host-side setup_reg (grid.f90:142-230): for every face within 1.5*delta of a
+// body point (box test), weight delta^2 * d(x-xb) * d(y-yb). Faces near each
+// point are enumerated directly instead of scanning all Nq faces; per-face
+// entry order stays the reference's (ascending body point), and per-force
+// entries are by ascending face index, the order of regT's scatter loop.
+static void setup_reg_host(HostCase& c) {
+  int m = c.m, n = c.n, nb = c.nb;
+  double delta = c.delta, d2 = 0.5 * delta, sup = 3.0 * d2;
+  double ox = c.p.offsetx, oy = c.p.offsety;
+  struct Ent { int face, force; double w; };
+  std::vector<Ent> ents;
+  for (int k = 0; k < nb; k++) {
+    double xk = c.xb[k], yk = c.yb[k];
+    // u faces: x = delta*(i-1)-ox, y = delta*(j-1)-oy+d2
+    int i0 = std::max(1, (int)std::floor((xk + ox - sup) / delta) + 1 - 1);
+    int i1 = std::min(m + 1, (int)std::ceil((xk + ox + sup) / delta) + 1 + 1);
+    int j0 = std::max(1, (int)std::floor((yk + oy - d2 - sup) / delta) + 1 - 1);
+    int j1 = std::min(n, (int)std::ceil((yk + oy - d2 + sup) / delta) + 1 + 1);
+    for (int i = i0; i <= i1; i++)
+      for (int j = j0; j <= j1; j++) {
+        double x = delta * (double)(i - 1) - ox;
+        double y = delta * (double)(j - 1) - oy + d2;
+        if (std::fabs(x - xk) < sup && std::fabs(y - yk) < sup)
+          ents.push_back({(i - 1) + (j - 1) * (m + 1), k,
+                          (delta * delta) * deltafnc(x, xk, delta) * deltafnc(y, yk, delta)});
+      }
+    // v faces: x = delta*(i-1)-ox+d2, y = delta*(j-1)-oy
+    i0 = std::max(1, (int)std::floor((xk + ox - d2 - sup) / delta) + 1 - 1);
+    i1 = std::min(m, (int)std::ceil((xk + ox - d2 + sup) / delta) + 1 + 1);
+    j0 = std::max(1, (int)std::floor((yk + oy - sup) / delta) + 1 - 1);
+    j1 = std::min(n + 1, (int)std::ceil((yk + oy + sup) / delta) + 1 + 1);
+    for (int i = i0; i <= i1; i++)
+      for (int j = j0; j <= j1; j++) {
+        double x = delta * (double)(i - 1) - ox + d2;
+        double y = delta * (double)(j - 1) - oy;
+        if (std::fabs(x - xk) < sup && std::fabs(y - yk) < sup)
+          ents.push_back({(m + 1) * n + (i - 1) + (j - 1) * m, nb + k,
+                          (delta * delta) * deltafnc(x, xk, delta) * deltafnc(y, yk, delta)});
+      }
+  }
+  // CSR by face, entries in ascending body-point order (stable sort by face)
+  std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) { return a.face < b.face; });
+  c.face_ptr.assign(c.nq + 1, 0);
+  c.face_f.clear();
+  c.face_w.clear();
+  for (auto& e : ents) c.face_ptr[e.face + 1]++;
+  for (int f = 0; f < c.nq; f++) c.face_ptr[f + 1] += c.face_ptr[f];
+  for (auto& e : ents) {
+    c.face_f.push_back(e.force);
+    c.face_w.push_back(e.w);
+  }
+  // CSR by force, faces ascending (ents is face-sorted; stable by force)
+  std::vector<Ent> byf = ents;
+  std::stable_sort(byf.begin(), byf.end(), [](const Ent& a, const Ent& b) { return a.force < b.force; });
+  c.force_ptr.assign(c.nf + 1, 0);
+  c.force_face.clear();
+  c.force_w.clear();
+  for (auto& e : byf) c.force_ptr[e.force + 1]++;
+  for (int f = 0; f < c.nf; f++) c.force_ptr[f + 1] += c.force_ptr[f];
+  c.wsum.assign(c.nf, 0.0);
+  for (auto& e : byf) {
+    c.force_face.push_back(e.face);
+    c.force_w.push_back(e.w);
+    c.wsum[e.force] += e.w;
+  }
+}
+
+static double* sine_matrix(ibfs_handle* h, int m) {
+  auto it = h->sine.find(m);
+  if (it != h->sine.end()) return it->second;
+  int N = m - 1;
+  std::vector<double> S((size_t)N * N);
+  for (int a = 0; a < N; a++)
+    for (int b = 0; b < N; b++) {
+      long long p = ((long long)(a + 1) * (b + 1)) % (2 * m);
+      S[a + (size_t)b * N] = 2.0 * std::sin(M_PI * (double)p / (double)m);
+    }
+  double* d = dupload(h, S);
+  h->sine[m] = d;
+  return d;
+}
+
+static double* cos_table(ibfs_handle* h, int m) {
+  auto it = h->costab.find(m);
+  if (it != h->costab.end()) return it->second;
+  const double pi = 3.1415926535897932384;
+  std::vector<double> c(m - 1);
+  for (int i = 1; i <= m - 1; i++) c[i - 1] = std::cos(pi * (double)i / (double)m);
+  double* d = dupload(h, c);
+  h->costab[m] = d;
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// Step program construction
+struct ProgBuilder {
+  ibfs_handle* h;
+  std::vector<std::function<void()>>& P;
+  int cfg_for(const std::vector<GemmDesc>& ds) {
+    if (h->tile_cfg >= 0) return h->tile_cfg;
+    long tiles64 = 0;
+    for (auto& d : ds) tiles64 += gemm_tiles(d.M, d.N, 0);
+    return tiles64 >= 2 * 148 ? 0 : 1;
+  }
+  void gemm(std::vector<GemmDesc> ds, bool dual) {
+    if (ds.empty()) return;
+    int cfg = cfg_for(ds);
+    int mt = 0;
+    for (auto& d : ds) mt = std::max(mt, gemm_tiles(d.M, d.N, cfg));
+    GemmDesc* dd = dupload(h, ds);
+    int nd = (int)ds.size();
+    cudaStream_t st = h->st;
+    P.push_back([=]() { launch_gemm_f64(dd, nd, mt, cfg, dual, st); });
+  }
+  const LevelItem* items(const std::vector<LevelItem>& v) { return dupload(h, v); }
+  const int* ints(const std::vector<int>& v) { return dupload(h, v); }
+};
+
+static GemmDesc right_desc(const DevCase& c, const double* A, double* C) {
+  GemmDesc d{};
+  d.A = A; d.B = c.Sn; d.C = C;
+  d.M = c.m - 1; d.N = c.n - 1; d.K = c.n - 1;
+  d.lda = c.m - 1; d.ldb = c.n - 1; d.ldc = c.m - 1;
+  d.m = c.m; d.n = c.n;
+  d.cosx = c.cosx; d.cosy = c.cosy;
+  d.dt = c.dt; d.re = c.re; d.norm = c.norm;
+  return d;
+}
+static GemmDesc left_desc(const DevCase& c, const double* B, double* C, int epi, int k) {
+  GemmDesc d{};
+  d.A = c.Sm; d.B = B; d.C = C;
+  d.M = c.m - 1; d.N = c.n - 1; d.K = c.m - 1;
+  d.lda = c.m - 1; d.ldb = c.m - 1; d.ldc = c.m - 1;
+  d.m = c.m; d.n = c.n; d.k = k;
+  d.epi = epi;
+  d.cosx = c.cosx; d.cosy = c.cosy;
+  d.dt = c.dt; d.re = c.re; d.norm = c.norm;
+  d.del22 = c.delta * c.delta * std::pow(4.0, k - 1);
+  return d;
+}
+
+// vort2flux (operators.f90:191-240) over the given cases (host copies + their
+// index in the device case array). curl_all: curl on every level (nlev = L),
+// else on level 1 only (nlev = 1).
+static void build_vort2flux(ProgBuilder& B, const DevCase* dcases, const std::vector<DevCase>& cs,
+                            const std::vector<int>& ids, bool curl_all) {
+  ibfs_handle* h = B.h;
+  cudaStream_t st = h->st;
+  int Lmax = 0, mns = 0, mnq = 0;
+  for (auto& c : cs) { Lmax = std::max(Lmax, c.L); mns = std::max(mns, c.ns); mnq = std::max(mnq, c.nq); }
+  for (int k = 2; k <= Lmax; k++) {
+    std::vector<LevelItem> it;
+    for (size_t i = 0; i < cs.size(); i++) if (cs[i].L >= k) it.push_back({ids[i], k});
+    if (it.empty()) continue;
+    const LevelItem* d = B.items(it);
+    int ni = (int)it.size();
+    B.P.push_back([=]() { launch_coarsify(dcases, d, ni, mns, st); });
+  }
+  for (int t = 0; t < Lmax; t++) {
+    std::vector<GemmDesc> r1, l1, r2, l2;
+    for (size_t i = 0; i < cs.size(); i++) {
+      const DevCase& c = cs[i];
+      int k = c.L - t;
+      if (k < 1) continue;
+      double* om = c.omega + (size_t)(k - 1) * c.ns;
+      GemmDesc d = right_desc(c, om, c.wa);
+      if (k < c.L) { d.pro = PRO_APPLY_BC; d.bcsrc = c.s + (size_t)k * c.ns; }
+      r1.push_back(d);
+      l1.push_back(left_desc(c, c.wa, c.wb, EPI_LAMINV, k));
+      r2.push_back(right_desc(c, c.wb, c.wa));
+      l2.push_back(left_desc(c, c.wa, c.s + (size_t)(k - 1) * c.ns, EPI_STORE, k));
+    }
+    B.gemm(r1, false);
+    B.gemm(l1, false);
+    B.gemm(r2, false);
+    B.gemm(l2, false);
+  }
+  std::vector<LevelItem> ci;
+  for (size_t i = 0; i < cs.size(); i++)
+    for (int k = 1; k <= (curl_all ? cs[i].L : 1); k++) ci.push_back({ids[i], k});
+  const LevelItem* d = B.items(ci);
+  int ni = (int)ci.size();
+  B.P.push_back([=]() { launch_curl(dcases, d, ni, mnq, st); });
+}
+
+// ainv(x) on level 1 (myfft.f90:112-124): x in c.vort, result stored (or
+// subtracted) into omega level 1.
+static void build_ainv(ProgBuilder& B, const std::vector<DevCase>& cs, int final_epi) {
+  std::vector<GemmDesc> r1, l1, r2, l2;
+  for (auto& c : cs) {
+    r1.push_back(right_desc(c, c.vort, c.wa));
+    l1.push_back(left_desc(c, c.wa, c.wb, EPI_AINV, 1));
+    r2.push_back(right_desc(c, c.wb, c.wa));
+    l2.push_back(left_desc(c, c.wa, c.omega, final_epi, 1));
+  }
+  B.gemm(r1, false);
+  B.gemm(l1, false);
+  B.gemm(r2, false);
+  B.gemm(l2, false);
+}
+
+static void build_step_program(ibfs_handle* h) {
+  h->prog.clear();
+  ProgBuilder B{h, h->prog};
+  cudaStream_t st = h->st;
+  const DevCase* dcases = h->d_cases;
+  std::vector<DevCase> cs;
+  std::vector<int> ids;
+  for (size_t i = 0; i < h->cases.size(); i++) { cs.push_back(h->cases[i].dc); ids.push_back((int)i); }
+  int nc = (int)cs.size();
+  int Lmax = h->max_L, mns = h->max_ns, mnf = h->max_nf, mring = h->max_ring;
+  const int* d_ids = B.ints(ids);
+  h->prog.push_back([=]() { launch_step_begin(dcases, nc, st); });
+  // STEP 1 (operators.f90:97-134)
+  std::vector<LevelItem> all;
+  for (int i = 0; i < nc; i++) for (int k = 1; k <= cs[i].L; k++) all.push_back({i, k});
+  const LevelItem* d_all = B.items(all);
+  int nall = (int)all.size();
+  h->prog.push_back([=]() { launch_lastbc(dcases, d_all, nall, mring, st); });
+  if (h->precision == 1) {
+    build_precision_step1(h->prec, B.P, dcases, cs, st);
+  } else {
+    for (int t = 0; t < Lmax; t++) {
+      std::vector<LevelItem> it;
+      std::vector<GemmDesc> r1, l1, r2, l2;
+      for (int i = 0; i < nc; i++) {
+        const DevCase& c = cs[i];
+        int k = c.L - t;
+        if (k < 1) continue;
+        it.push_back({i, k});
+        double* om = c.omega + (size_t)(k - 1) * c.ns;
+        r1.push_back(right_desc(c, c.rhsA, c.wa));
+        r1.push_back(right_desc(c, om, c.wb));
+        GemmDesc cn = left_desc(c, c.wa, c.wc, EPI_CN, k);
+        cn.B2 = c.wb;
+        l1.push_back(cn);
+        r2.push_back(right_desc(c, c.wc, c.wa));
+        l2.push_back(left_desc(c, c.wa, om, EPI_STORE, k));
+      }
+      const LevelItem* d = B.items(it);
+      int ni = (int)it.size();
+      h->prog.push_back([=]() { launch_rhs(dcases, d, ni, mns, 0, st); });
+      B.gemm(r1, false);
+      B.gemm(l1, true);
+      B.gemm(r2, false);
+      B.gemm(l2, false);
+    }
+  }
+  // STEP 2 (operators.f90:142-171)
+  if (h->precision == 1) build_precision_vort2flux(h->prec, B.P, dcases, cs, ids, false, st);
+  else build_vort2flux(B, dcases, cs, ids, false);
+  h->prog.push_back([=]() { launch_rhsf(dcases, d_ids, nc, mnf, st); });
+  h->prog.push_back([=]() { launch_chol_solve(dcases, d_ids, nc, mnf, st); });
+  // STEP 3 (operators.f90:174)
+  h->prog.push_back([=]() { launch_regrot(dcases, d_ids, nc, mns, st); });
+  if (h->precision == 1) build_precision_ainv(h->prec, B.P, dcases, cs, EPI_SUBTRACT, st);
+  else build_ainv(B, cs, EPI_SUBTRACT);
+  // STEP 4 (operators.f90:177)
+  if (h->precision == 1) build_precision_vort2flux(h->prec, B.P, dcases, cs, ids, true, st);
+  else build_vort2flux(B, dcases, cs, ids, true);
+  // outputs (operators.f90:184-186)
+  std::vector<int> base;
+  int acc = 0;
+  for (int i = 0; i < nc; i++) { base.push_back(acc); acc += cs[i].L; }
+  const int* d_base = B.ints(base);
+  double* part = h->d_partial;
+  h->prog.push_back([=]() { launch_outputs(dcases, d_all, nall, d_ids, d_base, nc, part, st); });
+}
+
+static int capture_graph(ibfs_handle* h) {
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  h->graph_ok = false;
+  cudaGraph_t g;
+  if (cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return 0;
+  for (auto& f : h->prog) f();
+  if (cudaStreamEndCapture(h->st, &g) != cudaSuccess) { cudaGetLastError(); return 0; }
+  if (cudaGraphInstantiate(&h->gexec, g, 0) == cudaSuccess) h->graph_ok = true;
+  else cudaGetLastError();
+  cudaGraphDestroy(g);
+  return 0;
+}
+
+static int run_step(ibfs_handle* h) {
+  if (h->graph_ok) IBFS_CUDA_CHECK(cudaGraphLaunch(h->gexec, h->st));
+  else for (auto& f : h->prog) f();
+  IBFS_CUDA_CHECK(cudaGetLastError());
+  return IBFS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// preprocess: a_times on unit vectors in chunks of shadow cases.
+static int precompute(ibfs_handle* h) {
+  std::vector<int> need;
+  for (size_t i = 0; i < h->cases.size(); i++)
+    if (h->cases[i].p.stationary && !h->cases[i].have_chol && h->cases[i].nf > 0) need.push_back((int)i);
+  if (need.empty()) return IBFS_OK;
+  size_t budget = (size_t)4 << 30;
+  for (int ci : need) {
+    HostCase& hc = h->cases[ci];
+    const DevCase& c = hc.dc;
+    size_t per = sizeof(double) * ((size_t)(2 * c.L + 4) * c.ns + c.nq + c.nf);
+    int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)c.nf, budget / per));
+    // shadow pool
+    double *pom, *ps, *pw, *pq, *pf;
+    size_t nsL = (size_t)c.L * c.ns;
+    if (cudaMalloc(&pom, sizeof(double) * nsL * chunk) != cudaSuccess ||
+        cudaMalloc(&ps, sizeof(double) * nsL * chunk) != cudaSuccess ||
+        cudaMalloc(&pw, sizeof(double) * 4 * c.ns * chunk) != cudaSuccess ||
+        cudaMalloc(&pq, sizeof(double) * c.nq * chunk) != cudaSuccess ||
+        cudaMalloc(&pf, sizeof(double) * c.nf * chunk) != cudaSuccess)
+      return fail(IBFS_ERR_NOMEM, "device allocation failed in preprocess");
+    std::vector<void*> tmp_allocs;
+    int rc = IBFS_OK;
+    for (int j0 = 0; j0 < c.nf && rc == IBFS_OK; j0 += chunk) {
+      int nr = std::min(chunk, c.nf - j0);
+      std::vector<DevCase> sh(nr, c);
+      std::vector<int> ids(nr), cols(nr);
+      std::vector<double*> outs(nr);
+      for (int r = 0; r < nr; r++) {
+        DevCase& s = sh[r];
+        s.omega = pom + nsL * r;
+        s.s = ps + nsL * r;
+        s.wa = pw + (size_t)4 * c.ns * r;
+        s.wb = s.wa + c.ns;
+        s.wc = s.wb + c.ns;
+        s.vort = s.wc + c.ns;
+        s.q = pq + (size_t)c.nq * r;
+        s.fb = pf + (size_t)c.nf * r;
+        ids[r] = r;
+        cols[r] = j0 + r;
+        outs[r] = c.chol + (size_t)(j0 + r) * c.nf;  // cholmat(:, j) = a_times(e_j)
+      }
+      std::vector<std::function<void()>> P;
+      ibfs_handle tmp;  // collects this chunk's uploads
+      ProgBuilder B{&tmp, P};
+      DevCase* dsh = dupload(&tmp, sh);
+      const int* dids = B.ints(ids);
+      const int* dcols = B.ints(cols);
+      double** douts = dupload(&tmp, outs);
+      cudaStream_t st = h->st;
+      int mnf = c.nf, mns = c.ns;
+      cudaMemsetAsync(pom, 0, sizeof(double) * nsL * nr, st);
+      P.push_back([=]() { launch_unit_fb(dsh, dids, dcols, nr, mnf, st); });
+      P.push_back([=]() { launch_regrot(dsh, dids, nr, mns, st); });
+      tmp.tile_cfg = h->tile_cfg;
+      tmp.st = st;
+      // A is always built in FP64 (the force system stays FP64 in every form)
+      build_ainv(B, sh, EPI_STORE);
+      build_vort2flux(B, dsh, sh, ids, false);
+      P.push_back([=]() { launch_regT_out(dsh, dids, nr, mnf, douts, st); });
+      for (auto& f : P) {
+        f();
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) { rc = fail_cuda(le, "preprocess launch"); break; }
+      }
+      cudaError_t e = cudaStreamSynchronize(st);
+      if (rc == IBFS_OK && e != cudaSuccess) rc = fail_cuda(e, "preprocess a_times");
+      for (void* p : tmp.allocs) cudaFree(p);
+      tmp.allocs.clear();
+    }
+    cudaFree(pom); cudaFree(ps); cudaFree(pw); cudaFree(pq); cudaFree(pf);
+    if (rc) return rc;
+    std::vector<int> one{ci};
+    int* dcid = dupload(h, one);
+    IBFS_CUDA_CHECK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
+    launch_chol_factor(h->d_cases, dcid, 1, h->d_status, h->st);
+    int status = 0;
+    IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+    if (status) return fail(IBFS_ERR_CHOL, "choldc failed");
+    launch_chol_inverse(h->d_cases, dcid, 1, h->st);
+    IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+    hc.have_chol = true;
+  }
+  return IBFS_OK;
+}
+
+static int refresh_inverse(ibfs_handle* h, int ci) {
+  std::vector<int> one{ci};
+  int* dcid = dupload(h, one);
+  launch_chol_inverse(h->d_cases, dcid, 1, h->st);
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  return IBFS_OK;
+}
+
+static int setup_case(ibfs_handle* h, HostCase& c, const ibfs_params_c& p, const ibfs_options_c* o, int nb,
+                      const double* xb, const double* yb, const int* bdyno) {
+  c.p = p;
+  if (o) c.o = *o; else { memset(&c.o, 0, sizeof(c.o)); c.o.tile_cfg = -1; }
+  if (p.m % 4 != 0 || p.n % 4 != 0 || p.m < 8 || p.n < 8)
+    return fail(IBFS_ERR_GRID, "HEY! Grid nodes must be divisible by 4!!");
+  c.m = p.m; c.n = p.n;
+  c.delta = p.len / (double)p.m;
+  int nlm = nlevmax(p.m, p.n);
+  c.L = std::max(1, std::min(p.mgridlev, nlm));
+  c.p.mgridlev = c.L;
+  c.ns = (c.m - 1) * (c.n - 1);
+  c.nq = (c.m + 1) * c.n + (c.n + 1) * c.m;
+  c.nb = nb; c.nf = 2 * nb;
+  c.nring = 2 * (c.m + 1) + 2 * (c.n + 1);
+  c.norm = 4.0 * (double)(float)((long long)c.m * c.n);
+  c.xb.assign(xb, xb + nb);
+  c.yb.assign(yb, yb + nb);
+  c.bdyno.assign(nb, 0);
+  if (bdyno) c.bdyno.assign(bdyno, bdyno + nb);
+  int bmin = 0, bmax = 0;
+  for (int k = 0; k < nb; k++) {
+    if (k == 0 || c.bdyno[k] < bmin) bmin = c.bdyno[k];
+    if (k == 0 || c.bdyno[k] > bmax) bmax = c.bdyno[k];
+  }
+  c.bmin = bmin;
+  c.nbody = nb ? bmax - bmin + 1 : 0;
+  if (c.nbody > 64) return fail(IBFS_ERR_ARG, "at most 64 bodies per case");
+  c.itime = p.istart;
+  setup_reg_host(c);
+  DevCase& d = c.dc;
+  d.m = c.m; d.n = c.n; d.L = c.L; d.ns = c.ns; d.nq = c.nq; d.nb = c.nb; d.nf = c.nf; d.nring = c.nring;
+  d.nbody = c.nbody; d.bmin = c.bmin;
+  d.delta = c.delta; d.dt = p.dt; d.re = p.re; d.norm = c.norm;
+  size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
+  d.omega = dalloc<double>(h, nsL);
+  d.rhs_old = dalloc<double>(h, nsL);
+  d.q = dalloc<double>(h, nqL);
+  d.q0 = dalloc<double>(h, nqL);
+  d.fb = dalloc<double>(h, c.nf);
+  d.s = dalloc<double>(h, nsL);
+  d.lastbc = dalloc<double>(h, (size_t)c.L * c.nring);
+  d.rhsA = dalloc<double>(h, c.ns);
+  d.wa = dalloc<double>(h, c.ns);
+  d.wb = dalloc<double>(h, c.ns);
+  d.wc = dalloc<double>(h, c.ns);
+  d.wd = dalloc<double>(h, c.ns);
+  d.vort = dalloc<double>(h, c.ns);
+  d.cosx = cos_table(h, c.m);
+  d.cosy = cos_table(h, c.n);
+  d.Sm = sine_matrix(h, c.m);
+  d.Sn = sine_matrix(h, c.n);
+  d.rhsf = dalloc<double>(h, c.nf);
+  d.motion = dalloc<double>(h, c.nf);
+  d.fwork = dalloc<double>(h, c.nf);
+  d.bvel = dalloc<double>(h, c.nf);
+  d.face_ptr = dupload(h, c.face_ptr);
+  d.face_f = dupload(h, c.face_f);
+  d.face_w = dupload(h, c.face_w);
+  d.force_ptr = dupload(h, c.force_ptr);
+  d.force_face = dupload(h, c.force_face);
+  d.force_w = dupload(h, c.force_w);
+  d.wsum = dupload(h, c.wsum);
+  d.bdyno = dupload(h, c.bdyno);
+  d.Linv = dalloc<double>(h, (size_t)c.nf * c.nf);
+  d.LinvT = dalloc<double>(h, (size_t)c.nf * c.nf);
+  d.chol = dalloc<double>(h, (size_t)c.nf * c.nf + c.nf);
+  if (!d.omega || !d.q || !d.s || !d.chol || !d.Sm || !d.Sn) return fail(IBFS_ERR_NOMEM, "device allocation failed");
+  // initial state (variables.f90:55-64)
+  if (p.unif_flow) {
+    std::vector<double> q0(nqL, 0.0);
+    for (int k = 1; k <= c.L; k++)
+      for (size_t t = 0; t < (size_t)(c.m + 1) * c.n; t++) q0[t + (k - 1) * c.nq] = c.delta * std::pow(2.0, k - 1);
+    cudaMemcpy(d.q0, q0.data(), sizeof(double) * nqL, cudaMemcpyHostToDevice);
+  }
+  return IBFS_OK;
+}
+
+static int finish_create(ibfs_handle* h) {
+  gemm_f64_init();
+  IBFS_CUDA_CHECK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  IBFS_CUDA_CHECK(cudaEventCreate(&h->ev0));
+  IBFS_CUDA_CHECK(cudaEventCreate(&h->ev1));
+  int nc = (int)h->cases.size();
+  h->d_itime = dalloc<int>(h, nc);
+  h->d_status = dalloc<int>(h, 4);
+  int off = 0;
+  for (int i = 0; i < nc; i++) {
+    HostCase& c = h->cases[i];
+    c.out_off = off;
+    off += 2 * c.nbody + c.L + 1;
+    h->max_ns = std::max(h->max_ns, c.ns);
+    h->max_nq = std::max(h->max_nq, c.nq);
+    h->max_nf = std::max(h->max_nf, c.nf);
+    h->max_ring = std::max(h->max_ring, c.nring);
+    h->max_L = std::max(h->max_L, c.L);
+  }
+  h->out_stride = off;
+  h->d_out = dalloc<double>(h, off);
+  int nitems = 0;
+  for (auto& c : h->cases) nitems += c.L;
+  h->d_partial = dalloc<double>(h, (size_t)nitems * 32);
+  std::vector<int> it0(nc);
+  for (int i = 0; i < nc; i++) {
+    HostCase& c = h->cases[i];
+    c.dc.out = h->d_out + c.out_off;
+    c.dc.itime = h->d_itime + i;
+    c.dc.status = h->d_status;
+    it0[i] = c.itime;
+  }
+  cudaMemcpy(h->d_itime, it0.data(), sizeof(int) * nc, cudaMemcpyHostToDevice);
+  std::vector<DevCase> dcs;
+  for (auto& c : h->cases) dcs.push_back(c.dc);
+  h->d_cases = dupload(h, dcs);
+  if (!h->d_cases || !h->d_out) return fail(IBFS_ERR_NOMEM, "device allocation failed");
+  if (cudaMallocHost(&h->h_stage, sizeof(double) * std::max(off, h->max_nf) * 2) != cudaSuccess)
+    return fail(IBFS_ERR_NOMEM, "pinned allocation failed");
+  if (h->precision == 1) {
+    int rc = precision_init(h->prec, h->st, dcs, h->d_cases, [h](size_t bytes) -> void* {
+      void* p = nullptr;
+      if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+      cudaMemset(p, 0, bytes);
+      h->allocs.push_back(p);
+      return p;
+    });
+    if (rc) return fail(rc, precision_error());
+  }
+  build_step_program(h);
+  IBFS_CUDA_CHECK(cudaDeviceSynchronize());
+  capture_graph(h);
+  IBFS_CUDA_CHECK(cudaGetLastError());
+  return IBFS_OK;
+}
+
+static void free_handle(ibfs_handle* h) {
+  if (!h) return;
+  if (h->st) cudaStreamSynchronize(h->st);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->st) cudaStreamDestroy(h->st);
+  if (h->prec) precision_free(h->prec);
+  delete h;
+}
+
+static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out);
+
+}  // namespace ibfs
+
+// ===========================================================================
+// C-ABI
+extern "C" {
+
+int ibfs_batch_create(int ncases, const ibfs_params_c* p, const ibfs_options_c* opt, const int* nb,
+                      const double* xb, const double* yb, const int* bdyno, ibfs_handle** out) {
+  if (!out || !p || !nb || ncases < 1) return fail(IBFS_ERR_ARG, "null argument");
+  *out = nullptr;
+  ibfs_handle* h = new ibfs_handle();
+  h->precision = opt ? opt[0].precision : 0;
+  h->tile_cfg = opt ? opt[0].tile_cfg : -1;
+  if (opt && opt[0].tile_cfg == 0 && opt[0].precision == 0 && opt[0].cg_relative == 0 && opt[0].motion_kind == 0)
+    h->tile_cfg = -1;  // zero-initialised options mean "auto"
+  h->cases.resize(ncases);
+  size_t off = 0;
+  for (int i = 0; i < ncases; i++) {
+    int rc = setup_case(h, h->cases[i], p[i], opt ? &opt[i] : nullptr, nb[i], xb + off, yb + off,
+                        bdyno ? bdyno + off : nullptr);
+    off += nb[i];
+    if (rc) { std::string e = t_error; free_handle(h); t_error = e; return rc; }
+  }
+  int rc = finish_create(h);
+  if (rc) { std::string e = t_error; free_handle(h); t_error = e; return rc; }
+  *out = h;
+  return IBFS_OK;
+}
+
+int ibfs_create(const ibfs_params_c* p, const ibfs_options_c* opt, int nb, const double* xb, const double* yb,
+                const int* bdyno, ibfs_handle** out) {
+  return ibfs_batch_create(1, p, opt, &nb, xb, yb, bdyno, out);
+}
+
+int ibfs_destroy(ibfs_handle* h) {
+  free_handle(h);
+  return IBFS_OK;
+}
+
+int ibfs_num_cases(const ibfs_handle* h) { return h ? (int)h->cases.size() : 0; }
+
+int ibfs_case_sizes(const ibfs_handle* h, int icase, int* m, int* n, int* nlev, int* nq, int* nb, int* nbody) {
+  if (!h || icase < 0 || icase >= (int)h->cases.size()) return IBFS_ERR_ARG;
+  const HostCase& c = h->cases[icase];
+  if (m) *m = c.m;
+  if (n) *n = c.n;
+  if (nlev) *nlev = c.L;
+  if (nq) *nq = c.nq;
+  if (nb) *nb = c.nb;
+  if (nbody) *nbody = c.nbody;
+  return IBFS_OK;
+}
+
+int ibfs_set_state(ibfs_handle* h, int icase, const double* omega, const double* fb, const double* rhs_old,
+                   const double* q, const double* q0) {
+  if (!h || icase < 0 || icase >= (int)h->cases.size()) return IBFS_ERR_ARG;
+  const HostCase& c = h->cases[icase];
+  size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
+  auto cp = [&](double* d, const double* s, size_t n) {
+    return s ? cudaMemcpyAsync(d, s, n * sizeof(double), cudaMemcpyHostToDevice, h->st) : cudaSuccess;
+  };
+  IBFS_CUDA_CHECK(cp(c.dc.omega, omega, nsL));
+  IBFS_CUDA_CHECK(cp(c.dc.fb, fb, c.nf));
+  IBFS_CUDA_CHECK(cp(c.dc.rhs_old, rhs_old, nsL));
+  IBFS_CUDA_CHECK(cp(c.dc.q, q, nqL));
+  IBFS_CUDA_CHECK(cp(c.dc.q0, q0, nqL));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  return IBFS_OK;
+}
+
+int ibfs_get_state(const ibfs_handle* h, int icase, double* omega, double* fb, double* rhs_old, double* q,
+                   double* q0) {
+  if (!h || icase < 0 || icase >= (int)h->cases.size()) return IBFS_ERR_ARG;
+  const HostCase& c = h->cases[icase];
+  size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
+  auto cp = [&](double* d, const double* s, size_t n) {
+    return d ? cudaMemcpyAsync(d, s, n * sizeof(double), cudaMemcpyDeviceToHost, h->st) : cudaSuccess;
+  };
+  IBFS_CUDA_CHECK(cp(omega, c.dc.omega, nsL));
+  IBFS_CUDA_CHECK(cp(fb, c.dc.fb, c.nf));
+  IBFS_CUDA_CHECK(cp(rhs_old, c.dc.rhs_old, nsL));
+  IBFS_CUDA_CHECK(cp(q, c.dc.q, nqL));
+  IBFS_CUDA_CHECK(cp(q0, c.dc.q0, nqL));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  return IBFS_OK;
+}
+
+int ibfs_set_cholesky(ibfs_handle* h, int icase, const double* cholmat, const double* cholvec) {
+  if (!h || icase < 0 || icase >= (int)h->cases.size() || !cholmat || !cholvec) return IBFS_ERR_ARG;
+  HostCase& c = h->cases[icase];
+  size_t nf = c.nf;
+  IBFS_CUDA_CHECK(cudaMemcpy(c.dc.chol, cholmat, nf * nf * sizeof(double), cudaMemcpyHostToDevice));
+  IBFS_CUDA_CHECK(cudaMemcpy(c.dc.chol + nf * nf, cholvec, nf * sizeof(double), cudaMemcpyHostToDevice));
+  int rc = refresh_inverse(h, icase);
+  if (rc) return rc;
+  c.have_chol = true;
+  return IBFS_OK;
+}
+
+int ibfs_get_cholesky(const ibfs_handle* h, int icase, double* cholmat, double* cholvec) {
+  if (!h || icase < 0 || icase >= (int)h->cases.size()) return IBFS_ERR_ARG;
+  const HostCase& c = h->cases[icase];
+  size_t nf = c.nf;
+  if (cholmat) IBFS_CUDA_CHECK(cudaMemcpy(cholmat, c.dc.chol, nf * nf * sizeof(double), cudaMemcpyDeviceToHost));
+  if (cholvec) IBFS_CUDA_CHECK(cudaMemcpy(cholvec, c.dc.chol + nf * nf, nf * sizeof(double), cudaMemcpyDeviceToHost));
+  return IBFS_OK;
+}
+
+int ibfs_precompute(ibfs_handle* h) {
+  if (!h) return IBFS_ERR_ARG;
+  int rc = precompute(h);
+  if (rc) h->err = t_error;
+  return rc;
+}
+
+int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx, double* fy, double* circ,
+                 double* slip) {
+  if (!h || !itime || h->cases.size() != 1) return fail(IBFS_ERR_ARG, "ibfs_advance needs a single-case handle");
+  HostCase& c = h->cases[0];
+  if (*itime != c.itime) {
+    c.itime = *itime;
+    IBFS_CUDA_CHECK(cudaMemcpyAsync(h->d_itime, itime, sizeof(int), cudaMemcpyHostToDevice, h->st));
+  }
+  if (*itime + 1 == 1 || !c.have_chol) {
+    int rc = precompute(h);
+    if (rc) { h->err = t_error; return rc; }
+  }
+  if (body_vel) {
+    memcpy(h->h_stage, body_vel, sizeof(double) * c.nf);
+    IBFS_CUDA_CHECK(cudaMemcpyAsync(c.dc.bvel, h->h_stage, sizeof(double) * c.nf, cudaMemcpyHostToDevice, h->st));
+  } else {
+    IBFS_CUDA_CHECK(cudaMemsetAsync(c.dc.bvel, 0, sizeof(double) * c.nf, h->st));
+  }
+  int rc = run_step(h);
+  if (rc) { h->err = t_error; return rc; }
+  double* o = h->h_stage + c.nf;
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(o, h->d_out, sizeof(double) * h->out_stride, cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  *itime += 1;
+  c.itime = *itime;
+  if (fx) memcpy(fx, o, sizeof(double) * c.nbody);
+  if (fy) memcpy(fy, o + c.nbody, sizeof(double) * c.nbody);
+  if (circ) memcpy(circ, o + 2 * c.nbody, sizeof(double) * c.L);
+  if (slip) *slip = o[2 * c.nbody + c.L];
+  return IBFS_OK;
+}
+
+int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist) {
+  if (!h || nsteps < 0) return IBFS_ERR_ARG;
+  bool need = false;
+  for (auto& c : h->cases) if (c.p.stationary && !c.have_chol) need = true;
+  if (need) {
+    int rc = precompute(h);
+    if (rc) { h->err = t_error; return rc; }
+  }
+  if (hist && h->hist_steps < nsteps) {
+    if (h->d_hist) cudaFree(h->d_hist);
+    if (cudaMalloc(&h->d_hist, sizeof(double) * (size_t)nsteps * h->out_stride) != cudaSuccess)
+      return fail(IBFS_ERR_NOMEM, "history allocation failed");
+    h->hist_steps = nsteps;
+  }
+  IBFS_CUDA_CHECK(cudaEventRecord(h->ev0, h->st));
+  for (int s = 0; s < nsteps; s++) {
+    int rc = run_step(h);
+    if (rc) { h->err = t_error; return rc; }
+    if (hist)
+      IBFS_CUDA_CHECK(cudaMemcpyAsync(h->d_hist + (size_t)s * h->out_stride, h->d_out,
+                                      sizeof(double) * h->out_stride, cudaMemcpyDeviceToDevice, h->st));
+  }
+  IBFS_CUDA_CHECK(cudaEventRecord(h->ev1, h->st));
+  if (hist)
+    IBFS_CUDA_CHECK(cudaMemcpyAsync(hist, h->d_hist, sizeof(double) * (size_t)nsteps * h->out_stride,
+                                    cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  for (auto& c : h->cases) c.itime += nsteps;
+  return IBFS_OK;
+}
+
+int ibfs_output_offset(const ibfs_handle* h, int icase) {
+  if (!h || icase < 0 || icase >= (int)h->cases.size()) return -1;
+  return h->cases[icase].out_off;
+}
+int ibfs_output_stride(const ibfs_handle* h) { return h ? h->out_stride : 0; }
+
+int ibfs_last_timing(const ibfs_handle* h, double* ms) {
+  if (!h || !ms) return IBFS_ERR_ARG;
+  *ms = h->last_ms;
+  return IBFS_OK;
+}
+
+int ibfs_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
+  if (!h || !in || !out) return IBFS_ERR_ARG;
+  int rc = run_apply_op(h, op, in, out);
+  if (rc) h->err = t_error;
+  return rc;
+}
+
+const char* ibfs_last_error(const ibfs_handle* h) {
+  if (h && !h->err.empty()) return h->err.c_str();
+  return t_error.c_str();
+}
+
+}  // extern "C"
+
+namespace ibfs {
+
+// Single-operator application on case 0 (verification entry point).
+static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
+  HostCase& hc = h->cases[0];
+  DevCase c = hc.dc;
+  cudaStream_t st = h->st;
+  std::vector<std::function<void()>> P;
+  ibfs_handle tmp;
+  tmp.st = st;
+  tmp.tile_cfg = h->tile_cfg;
+  ProgBuilder B{&tmp, P};
+  size_t ns = c.ns;
+  // private scratch so the case state is untouched
+  DevCase s = c;
+  s.omega = dalloc<double>(&tmp, (size_t)c.L * ns);
+  s.s = dalloc<double>(&tmp, (size_t)c.L * ns);
+  s.q = dalloc<double>(&tmp, (size_t)c.L * c.nq);
+  s.fb = dalloc<double>(&tmp, c.nf);
+  s.wa = dalloc<double>(&tmp, ns);
+  s.wb = dalloc<double>(&tmp, ns);
+  s.wc = dalloc<double>(&tmp, ns);
+  s.vort = dalloc<double>(&tmp, ns);
+  std::vector<DevCase> sv{s};
+  DevCase* ds = dupload(&tmp, sv);
+  std::vector<int> ids{0};
+  const int* dids = B.ints(ids);
+  int rc = IBFS_OK;
+  size_t in_n = 0, out_n = 0;
+  double* dout = nullptr;
+  if (op == 0 || op == 1 || op == 2) {
+    in_n = ns; out_n = ns;
+    IBFS_CUDA_CHECK(cudaMemcpy(s.vort, in, ns * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->precision == 1) {
+      rc = precision_apply_op(h->prec, op, ds, s, st);
+      dout = s.omega;
+    } else {
+      if (op == 0) {
+        B.gemm({right_desc(s, s.vort, s.wa)}, false);
+        B.gemm({left_desc(s, s.wa, s.omega, EPI_STORE, 1)}, false);
+      } else {
+        B.gemm({right_desc(s, s.vort, s.wa)}, false);
+        B.gemm({left_desc(s, s.wa, s.wb, op == 1 ? EPI_LAMINV : EPI_AINV, 1)}, false);
+        B.gemm({right_desc(s, s.wb, s.wa)}, false);
+        B.gemm({left_desc(s, s.wa, s.omega, EPI_STORE, 1)}, false);
+      }
+      dout = s.omega;
+    }
+  } else if (op == 3) {  // a_times
+    in_n = c.nf; out_n = c.nf;
+    IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
+    IBFS_CUDA_CHECK(cudaMemset(s.omega, 0, (size_t)c.L * ns * sizeof(double)));
+    P.push_back([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
+    if (h->precision == 1) build_precision_ainv(h->prec, P, ds, sv, EPI_STORE, st);
+    else build_ainv(B, sv, EPI_STORE);
+    if (h->precision == 1) build_precision_vort2flux(h->prec, P, ds, sv, ids, false, st);
+    else build_vort2flux(B, ds, sv, ids, false);
+    double** douts = nullptr;
+    std::vector<double*> o1{s.wc};
+    douts = dupload(&tmp, o1);
+    int nf = c.nf;
+    P.push_back([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
+    dout = s.wc;
+  } else if (op == 4) {  // regT
+    in_n = c.nq; out_n = c.nf;
+    IBFS_CUDA_CHECK(cudaMemcpy(s.q, in, c.nq * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double*> o1{s.wc};
+    double** douts = dupload(&tmp, o1);
+    int nf = c.nf;
+    P.push_back([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
+    dout = s.wc;
+  } else if (op == 5) {  // rot(reg(f))
+    in_n = c.nf; out_n = ns;
+    IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
+    P.push_back([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
+    dout = s.vort;
+  } else {
+    rc = fail(IBFS_ERR_ARG, "unknown op");
+  }
+  (void)in_n;
+  if (rc == IBFS_OK) {
+    for (auto& f : P) f();
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = fail_cuda(e, "apply_op");
+    else if (cudaMemcpy(out, dout, out_n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = fail(IBFS_ERR_CUDA, "copy out");
+  }
+  for (void* p : tmp.allocs) cudaFree(p);
+  tmp.allocs.clear();
+  return rc;
+}
+
+}  // namespace ibfs

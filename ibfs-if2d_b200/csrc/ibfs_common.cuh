@@ -1,0 +1,116 @@
+// ibfs_common.cuh -- device data layout and shared helpers of the B200 IBFS
+// advance (the per-timestep path of atchieu/ibfs-if2d, src/operators.f90).
+//
+// HBM layout (per case, one arena): every field keeps the reference's Fortran
+// column-major layout so state exchange is a plain copy:
+//   omega, rhs_old, s : [L][(m-1)*(n-1)]   node (i,j), i=2..m fastest
+//   q, q0             : [L][Nq]            u-faces u(i,j)=i+(j-1)(m+1), then
+//                                          v-faces v(i,j)=(m+1)n+i+(j-1)m
+//   fb, rhsf, motion  : [Nf]               x-forces then y-forces
+//   lastbc            : [L][nring]         ring left|right|bottom|top
+// Kernels are "grouped": they take a device array of items (case, level) so
+// one launch serves one case (plain form) or many uneven cases (batched form).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ibfs {
+
+struct DevCase {
+  int m, n, L, ns, nq, nb, nf, nring;
+  int nbody, bmin;
+  double delta, dt, re, norm;
+  // state
+  double *omega, *rhs_old, *q, *q0, *fb;
+  // per-level work
+  double *s;       // [L][ns] streamfunction per level
+  double *lastbc;  // [L][nring]
+  double *rhsA;    // [ns] combined right-hand side of the CN solve
+  double *wa, *wb, *wc, *wd;  // [ns] transform scratch
+  double *vort;    // [ns] scratch node field
+  // spectral tables (cos(pi i/m), cos(pi j/n)) and sine matrices
+  const double *cosx, *cosy;
+  const double *Sm, *Sn;  // 2 sin(pi a b / m), (m-1)x(m-1) col-major
+  // immersed boundary
+  double *rhsf, *motion, *fwork, *bvel;     // [Nf]
+  const int* face_ptr;  // [Nq+1] CSR by face: entries (force, weight) in reference k order
+  const int* face_f;
+  const double* face_w;
+  const int* force_ptr;  // [Nf+1] CSR by force: entries (face, weight) by ascending face
+  const int* force_face;
+  const double* force_w;
+  const double* wsum;    // [Nf] sum of a force's smear weights
+  const int* bdyno;      // [Nb]
+  double *Linv, *LinvT;  // [Nf*Nf] row-major inverse Cholesky factor and its transpose
+  double* chol;          // [Nf*Nf] cholmat (Fortran layout) and cholvec after it
+  // outputs of the last step
+  double* out;  // fx[nbody], fy[nbody], circ[L], slip
+  int* itime;   // device step counter
+  int* status;  // device error flags
+};
+
+struct LevelItem {
+  int c;  // case index
+  int k;  // level, 1-based
+};
+
+// Fortran-style index helpers. Node arrays are declared DIMENSION(2:m,2:n):
+__device__ __forceinline__ int nidx(int i, int j, int m) { return (i - 2) + (j - 2) * (m - 1); }
+// assumed-shape sections (lower bound 1), used by get_bc/apply_bc:
+__device__ __forceinline__ int ridx(int a, int b, int m) { return (a - 1) + (b - 1) * (m - 1); }
+// 0-based face offsets of u(i,j), v(i,j):
+__device__ __forceinline__ int uoff(int i, int j, int m) { return (i - 1) + (j - 1) * (m + 1); }
+__device__ __forceinline__ int voff(int i, int j, int m, int n) { return (m + 1) * n + (i - 1) + (j - 1) * m; }
+
+// Ring offsets (grid.f90:73-76).
+__device__ __forceinline__ int ring_left(int, int) { return 0; }
+__device__ __forceinline__ int ring_right(int, int n) { return n + 1; }
+__device__ __forceinline__ int ring_bottom(int, int n) { return 2 * (n + 1); }
+__device__ __forceinline__ int ring_top(int m, int n) { return 2 * (n + 1) + m + 1; }
+
+enum Side { SIDE_LEFT = 0, SIDE_RIGHT = 1, SIDE_BOTTOM = 2, SIDE_TOP = 3 };
+
+// get_bc (operators.f90:336-367) evaluated for one ring entry: the value the
+// reference stores at rbc(side + I), I = 1..m+1 (bottom/top) or 1..n+1
+// (left/right), before the final multiplication by fac. r is the coarser
+// level's node field (assumed shape, 1-based).
+__device__ __forceinline__ double getbc_raw(const double* __restrict__ r, int m, int n, int side, int I) {
+  int t = I - 1;  // loop variable i (or j) of get_bc
+  if (side == SIDE_BOTTOM || side == SIDE_TOP) {
+    int b = (side == SIDE_BOTTOM) ? n / 4 : 3 * n / 4;
+    if ((t & 1) == 0) return r[ridx(m / 4 + t / 2, b, m)];
+    return 0.5 * (r[ridx(m / 4 + (t + 1) / 2, b, m)] + r[ridx(m / 4 - 1 + (t + 1) / 2, b, m)]);
+  } else {
+    int a = (side == SIDE_LEFT) ? m / 4 : 3 * m / 4;
+    if ((t & 1) == 0) return r[ridx(a, n / 4 + t / 2, m)];
+    return 0.5 * (r[ridx(a, n / 4 + (t + 1) / 2, m)] + r[ridx(a, n / 4 - 1 + (t + 1) / 2, m)]);
+  }
+}
+
+__device__ __forceinline__ double ring_at(const double* __restrict__ ring, int m, int n, int side, int I) {
+  int off = side == SIDE_LEFT ? 0 : side == SIDE_RIGHT ? n + 1 : side == SIDE_BOTTOM ? 2 * (n + 1) : 2 * (n + 1) + m + 1;
+  return ring[off + I - 1];
+}
+
+// apply_bc (operators.f90:370-390) contribution to node r(a,b), added onto
+// val in the reference's order: bottom/top loop first, then left/right.
+// The ring value at side+I is supplied by a functor f(side, I).
+template <class F>
+__device__ __forceinline__ double apply_bc_at(double val, int a, int b, int m, int n, double fac, F f) {
+  if (b == 1) val = val + fac * f(SIDE_BOTTOM, a + 1);
+  if (b == n - 1) val = val + fac * f(SIDE_TOP, a + 1);
+  if (a == 1) val = val + fac * f(SIDE_LEFT, b + 1);
+  if (a == m - 1) val = val + fac * f(SIDE_RIGHT, b + 1);
+  return val;
+}
+
+// lam(i,j) of myfft.f90:131-132 from the cosine tables.
+__device__ __forceinline__ double lam_ij(double ci, double cj) { return -2.0 * (ci + cj - 2.0); }
+
+}  // namespace ibfs
+
+#define IBFS_CUDA_CHECK(x)                                  \
+  do {                                                      \
+    cudaError_t e_ = (x);                                   \
+    if (e_ != cudaSuccess) return ::ibfs::fail_cuda(e_, #x); \
+  } while (0)

@@ -1,0 +1,56 @@
+// ibfs_kernels.cuh -- launchers of the B200 IBFS kernels (host-callable).
+#pragma once
+#include "ibfs_common.cuh"
+
+namespace ibfs {
+
+// Dense-GEMM sine transform (one half of a 2-D DST-I, myfft.f90:83-94):
+//   C(M x N) = A(M x K) * B(K x N), column-major, FP64, with fused prologue
+//   (apply_bc of a coarser streamfunction, operators.f90:231-233) and
+//   epilogues for the spectral scalings of ctci / ainv / the CN update.
+enum GemmPro { PRO_NONE = 0, PRO_APPLY_BC = 1 };
+enum GemmEpi {
+  EPI_STORE = 0,     // C = acc
+  EPI_LAMINV = 1,    // C = laminv .* acc                    (ctci, myfft.f90:106)
+  EPI_AINV = 2,      // C = lam1i(:,:,1) .* acc / normalize  (ainv, myfft.f90:121)
+  EPI_CN = 3,        // C = lam1i_k .* (acc + lam1_k .* acc2)  (operators.f90:126-130)
+  EPI_SUBTRACT = 4,  // C = C - acc                          (operators.f90:174)
+};
+
+struct GemmDesc {
+  const double* A;
+  const double* B;
+  const double* B2;  // second right operand (EPI_CN)
+  double* C;
+  int M, N, K, lda, ldb, ldc;
+  int pro, epi;
+  int m, n, k;             // grid of the node field and its level
+  const double* bcsrc;     // PRO_APPLY_BC: coarser-level streamfunction
+  const double* cosx;      // cos(pi i/m), i=1..m-1
+  const double* cosy;      // cos(pi j/n), j=1..n-1
+  double dt, re, del22, norm;
+};
+
+void launch_gemm_f64(const GemmDesc* d_descs, int ndesc, int max_tiles, int tile_cfg, bool dual, cudaStream_t st);
+int gemm_tiles(int M, int N, int tile_cfg);
+void gemm_f64_init();
+
+void launch_lastbc(const DevCase* cases, const LevelItem* items, int nitems, int max_ring, cudaStream_t st);
+void launch_rhs(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, int first, cudaStream_t st);
+void launch_coarsify(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, cudaStream_t st);
+void launch_curl(const DevCase* cases, const LevelItem* items, int nitems, int max_nq, cudaStream_t st);
+void launch_regrot(const DevCase* cases, const int* cids, int ncases, int max_ns, cudaStream_t st);
+void launch_rhsf(const DevCase* cases, const int* cids, int ncases, int max_nf, cudaStream_t st);
+void launch_regT_out(const DevCase* cases, const int* cids, int ncases, int max_nf, double* const* outs,
+                     cudaStream_t st);
+void launch_unit_fb(const DevCase* cases, const int* cids, const int* cols, int ncases, int max_nf, cudaStream_t st);
+void launch_outputs(const DevCase* cases, const LevelItem* items, int nitems, const int* cids, const int* item_base,
+                    int ncases, double* partial, cudaStream_t st);
+void launch_step_begin(const DevCase* cases, int ncases, cudaStream_t st);
+
+// Cholesky factor / inverse / solve (operators.f90:766-819).
+void launch_chol_factor(const DevCase* cases, const int* cids, int ncases, int* status, cudaStream_t st);
+void launch_chol_inverse(const DevCase* cases, const int* cids, int ncases, cudaStream_t st);
+void launch_chol_solve(const DevCase* cases, const int* cids, int ncases, int max_nf, cudaStream_t st);
+
+}  // namespace ibfs

@@ -1,0 +1,30 @@
+// ibfs_precision.cuh -- split-precision form of the sine transforms: each DST
+// is a dense sine-matrix contraction on tcgen05 tensor cores with operands
+// split into three BF16 slices (FP32 accumulation), and every solve that uses
+// it gets one FP64 residual-correction sweep with the exact 5-point stencil.
+#pragma once
+#include <functional>
+#include <vector>
+
+#include "ibfs_common.cuh"
+#include "ibfs_kernels.cuh"
+
+namespace ibfs {
+
+struct PrecisionPlan;
+using Alloc = std::function<void*(size_t)>;
+using Prog = std::vector<std::function<void()>>;
+
+int precision_init(PrecisionPlan*& pp, cudaStream_t st, const std::vector<DevCase>& cases, const DevCase* d_cases,
+                   Alloc alloc);
+void precision_free(PrecisionPlan* pp);
+const char* precision_error();
+void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, const std::vector<DevCase>& cs,
+                           cudaStream_t st);
+void build_precision_vort2flux(PrecisionPlan* pp, Prog& P, const DevCase* dcases, const std::vector<DevCase>& cs,
+                               const std::vector<int>& ids, bool curl_all, cudaStream_t st);
+void build_precision_ainv(PrecisionPlan* pp, Prog& P, const DevCase* dcases, const std::vector<DevCase>& cs,
+                          int final_epi, cudaStream_t st);
+int precision_apply_op(PrecisionPlan* pp, int op, const DevCase* ds, const DevCase& s, cudaStream_t st);
+
+}  // namespace ibfs

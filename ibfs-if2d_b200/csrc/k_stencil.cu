@@ -1,0 +1,345 @@
+// k_stencil.cu -- HBM-bound stencil, inter-level and immersed-boundary kernels
+// of the IBFS advance. Each kernel follows the reference loop it replaces
+// (atchieu/ibfs-if2d src/operators.f90, cited per kernel); all arithmetic is
+// FP64. Grids are grouped: blockIdx.y selects a (case, level) item.
+#include "ibfs_common.cuh"
+#include "ibfs_kernels.cuh"
+
+namespace ibfs {
+
+// ---------------------------------------------------------------------------
+// lastbc(:,k) = get_bc(omega(:,:,k+1), 0.25) for k<L; lastbc(:,L) = 0
+// (operators.f90:97-100). One thread per ring entry.
+__global__ void k_lastbc(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items) {
+  LevelItem it = items[blockIdx.y];
+  const DevCase& C = cases[it.c];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C.nring) return;
+  int m = C.m, n = C.n;
+  double* ring = C.lastbc + (size_t)(it.k - 1) * C.nring;
+  if (it.k >= C.L) {
+    ring[t] = 0.0;
+    return;
+  }
+  int side, I;
+  if (t < n + 1) { side = SIDE_LEFT; I = t + 1; }
+  else if (t < 2 * (n + 1)) { side = SIDE_RIGHT; I = t - (n + 1) + 1; }
+  else if (t < 2 * (n + 1) + m + 1) { side = SIDE_BOTTOM; I = t - 2 * (n + 1) + 1; }
+  else { side = SIDE_TOP; I = t - 2 * (n + 1) - (m + 1) + 1; }
+  const double* r = C.omega + (size_t)it.k * C.ns;  // level k+1
+  ring[t] = getbc_raw(r, m, n, side, I) * 0.25;
+}
+
+// ---------------------------------------------------------------------------
+// Fused rhs of the per-level vorticity update (operators.f90:104-133):
+//   rhs    = rot(nonlinear(omega_k, q_k, q0_k, lastbc_k))       (:112, :465-510, :291-304)
+//   [first step] rhs_old = rhs                                   (:115-117)
+//   rhsbc  = apply_bc(lastbc_k)*vfac + apply_bc(omega_bc)*vfac   (:121-123)
+//   rhsA   = con1*rhs + con2*rhs_old + rhsbc                     (:127-129)
+//   rhs_old= rhs                                                 (:133)
+// omega_bc = get_bc(omega_{k+1}^new, 0.25) is gathered on the fly.
+__device__ __forceinline__ double vavg_at(const double* __restrict__ q, const double* __restrict__ q0, int i, int j,
+                                          int m, int n) {
+  int a = voff(i, j, m, n), b = voff(i - 1, j, m, n);
+  return 0.5 * (q[a] + q[b] + q0[a] + q0[b]);
+}
+__device__ __forceinline__ double uavg_at(const double* __restrict__ q, const double* __restrict__ q0, int i, int j,
+                                          int m) {
+  int a = uoff(i, j, m), b = uoff(i, j - 1, m);
+  return 0.5 * (q[a] + q[b] + q0[a] + q0[b]);
+}
+
+__global__ void k_rhs(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items, int first_step) {
+  LevelItem it = items[blockIdx.y];
+  const DevCase& C = cases[it.c];
+  int m = C.m, n = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C.ns) return;
+  int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
+  int k = it.k;
+  const double* om = C.omega + (size_t)(k - 1) * C.ns;
+  const double* q = C.q + (size_t)(k - 1) * C.nq;
+  const double* q0 = C.q0 + (size_t)(k - 1) * C.nq;
+  const double* bc = C.lastbc + (size_t)(k - 1) * C.nring;
+  int bottom = 2 * (n + 1), top = 2 * (n + 1) + m + 1, right = n + 1;
+  // omega extended with the ring along j (column i) and along i (row j)
+  auto Wj = [&](int jj) -> double {
+    if (jj == 1) return bc[bottom + i - 1];
+    if (jj == n + 1) return bc[top + i - 1];
+    return om[nidx(i, jj, m)];
+  };
+  auto Wi = [&](int ii, int jj) -> double {
+    if (ii == 1) return bc[jj - 1];
+    if (ii == m + 1) return bc[right + jj - 1];
+    return om[nidx(ii, jj, m)];
+  };
+  auto fqu = [&](int jj) -> double {  // fq(u(i,jj)), jj = 1..n
+    return 0.5 * (vavg_at(q, q0, i, jj + 1, m, n) * Wj(jj + 1) + vavg_at(q, q0, i, jj, m, n) * Wj(jj));
+  };
+  auto fqv = [&](int ii) -> double {  // fq(v(ii,j)), ii = 1..m
+    return -0.5 * (uavg_at(q, q0, ii + 1, j, m) * Wi(ii + 1, j) + uavg_at(q, q0, ii, j, m) * Wi(ii, j));
+  };
+  double rhs = fqv(i) - fqv(i - 1) - fqu(j) + fqu(j - 1);
+
+  double* ro = C.rhs_old + (size_t)(k - 1) * C.ns;
+  // explicit Euler on the first step (itime == 1), operators.f90:115-117
+  double rold = (first_step || *C.itime == 1) ? rhs : ro[t];
+  // rhsbc: two apply_bc passes onto zero, each in the reference's order
+  double vf = 0.5 * C.dt / C.re / (C.delta * C.delta * (double)(1 << (2 * (k - 1)))) / C.norm;
+  int a = i - 1, b = j - 1;
+  double rb = 0.0;
+  if (a == 1 || a == m - 1 || b == 1 || b == n - 1) {
+    rb = apply_bc_at(rb, a, b, m, n, vf, [&](int side, int I) { return ring_at(bc, m, n, side, I); });
+    if (k < C.L) {
+      const double* cr = C.omega + (size_t)k * C.ns;  // omega_{k+1}, already advanced
+      rb = apply_bc_at(rb, a, b, m, n, vf,
+                       [&](int side, int I) { return getbc_raw(cr, m, n, side, I) * 0.25; });
+    } else {
+      rb = apply_bc_at(rb, a, b, m, n, vf, [&](int, int) { return 0.0; });
+    }
+  }
+  double del22 = C.delta * C.delta * (double)(1 << (2 * (k - 1)));
+  double con1 = 1.5 * C.dt / del22 / C.norm;
+  double con2 = -0.5 * C.dt / del22 / C.norm;
+  C.rhsA[t] = con1 * rhs + con2 * rold + rb;
+  ro[t] = rhs;
+}
+
+// ---------------------------------------------------------------------------
+// coarsify (operators.f90:307-333), in place on level k from level k-1.
+__global__ void k_coarsify(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items) {
+  LevelItem it = items[blockIdx.y];
+  const DevCase& C = cases[it.c];
+  int m = C.m, n = C.n;
+  int ci = 3 * m / 4 - (m / 4 + 2) + 1, cj = 3 * n / 4 - (n / 4 + 2) + 1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ci * cj) return;
+  int i = t % ci + m / 4 + 2, j = t / ci + n / 4 + 2;
+  int ii = 2 * i - m / 2 - 1, jj = 2 * j - n / 2 - 1;
+  const double* f = C.omega + (size_t)(it.k - 2) * C.ns;
+  double* c = C.omega + (size_t)(it.k - 1) * C.ns;
+  auto R = [&](int x, int y) { return f[nidx(x, y, m)]; };
+  c[nidx(i, j, m)] = R(ii, jj) + 0.50 * (R(ii - 1, jj) + R(ii + 1, jj) + R(ii, jj - 1) + R(ii, jj + 1)) +
+                     0.25 * (R(ii - 1, jj - 1) + R(ii - 1, jj + 1) + R(ii + 1, jj - 1) + R(ii + 1, jj + 1));
+}
+
+// ---------------------------------------------------------------------------
+// curl (operators.f90:243-288) of s_k with sbc_k = get_bc(s_{k+1}, 1.0)
+// (operators.f90:231; zero on the coarsest level, :218) into q_k.
+__global__ void k_curl(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items) {
+  LevelItem it = items[blockIdx.y];
+  const DevCase& C = cases[it.c];
+  int m = C.m, n = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C.nq) return;
+  int k = it.k;
+  const double* x = C.s + (size_t)(k - 1) * C.ns;
+  const double* cs = (k < C.L) ? C.s + (size_t)k * C.ns : nullptr;
+  auto xbc = [&](int side, int I) -> double { return cs ? getbc_raw(cs, m, n, side, I) * 1.0 : 0.0; };
+  double v;
+  int nu = (m + 1) * n;
+  if (t < nu) {
+    int i = t % (m + 1) + 1, j = t / (m + 1) + 1;
+    if (i == 1) v = xbc(SIDE_LEFT, j + 1) - xbc(SIDE_LEFT, j);
+    else if (i == m + 1) v = xbc(SIDE_RIGHT, j + 1) - xbc(SIDE_RIGHT, j);
+    else if (j == 1) v = x[nidx(i, 2, m)] - xbc(SIDE_BOTTOM, i);
+    else if (j == n) v = xbc(SIDE_TOP, i) - x[nidx(i, n, m)];
+    else v = x[nidx(i, j + 1, m)] - x[nidx(i, j, m)];
+  } else {
+    int tv = t - nu;
+    int i = tv % m + 1, j = tv / m + 1;
+    if (j == 1) v = xbc(SIDE_BOTTOM, i) - xbc(SIDE_BOTTOM, i + 1);
+    else if (j == n + 1) v = xbc(SIDE_TOP, i) - xbc(SIDE_TOP, i + 1);
+    else if (i == 1) v = -x[nidx(2, j, m)] + xbc(SIDE_LEFT, j);
+    else if (i == m) v = -xbc(SIDE_RIGHT, j) + x[nidx(m, j, m)];
+    else v = x[nidx(i, j, m)] - x[nidx(i + 1, j, m)];
+  }
+  C.q[(size_t)(k - 1) * C.nq + t] = v;
+}
+
+// ---------------------------------------------------------------------------
+// vort = rot(reg(fb)) on level 1 (operators.f90:174 / :457, reg :513-528,
+// rot :291-304). reg is gathered per face from the CSR-by-face table whose
+// entries keep the reference's smear order.
+__device__ __forceinline__ double reg_face(const DevCase& C, const double* __restrict__ f, int face) {
+  int p0 = C.face_ptr[face], p1 = C.face_ptr[face + 1];
+  double h = 0.0;
+  for (int p = p0; p < p1; p++) h = h + C.face_w[p] * f[C.face_f[p]];
+  return h;
+}
+
+__global__ void k_regrot(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  int m = C.m, n = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C.ns) return;
+  int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
+  const double* f = C.fb;
+  double r = reg_face(C, f, voff(i, j, m, n)) - reg_face(C, f, voff(i - 1, j, m, n)) - reg_face(C, f, uoff(i, j, m)) +
+             reg_face(C, f, uoff(i, j - 1, m));
+  C.vort[t] = r;
+}
+
+// regT (operators.f90:531-546) of one face field, gathered per force in the
+// reference's scatter order (ascending face index).
+__device__ __forceinline__ double regT_force(const DevCase& C, const double* __restrict__ h, int f) {
+  int p0 = C.force_ptr[f], p1 = C.force_ptr[f + 1];
+  double s = 0.0;
+  for (int p = p0; p < p1; p++) s = s + C.force_w[p] * h[C.force_face[p]];
+  return s;
+}
+
+// motion = body velocity * delta - regT(q0(:,1));  rhsf = regT(q(:,1)) - motion
+// (operators.f90:142-164, grid.f90:573-574).
+__global__ void k_rhsf(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= C.nf) return;
+  double mot = (C.bvel ? C.bvel[f] * C.delta : 0.0) - regT_force(C, C.q0, f);
+  C.motion[f] = mot;
+  C.rhsf[f] = regT_force(C, C.q, f) - mot;
+}
+
+// a_times output column: out = regT(q(:,1)) (operators.f90:461).
+__global__ void k_regT_out(const DevCase* __restrict__ cases, const int* __restrict__ cids,
+                           double* const* __restrict__ outs) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= C.nf) return;
+  outs[blockIdx.y][f] = regT_force(C, C.q, f);
+}
+
+// Unit right-hand side e_j for the a_times columns (operators.f90:50-52).
+__global__ void k_unit_fb(const DevCase* __restrict__ cases, const int* __restrict__ cids, const int* __restrict__ cols) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= C.nf) return;
+  C.fb[f] = (f == cols[blockIdx.y]) ? 1.0 : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Per-step outputs (write_force :583-659 with xg = fb/dt, write_circ :662-699,
+// write_slip :549-580). Circulation is reduced in two fixed-order passes.
+constexpr int kCircBlocks = 32;
+
+__global__ void k_out_partial(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items,
+                              double* __restrict__ partial) {
+  LevelItem it = items[blockIdx.y];
+  const DevCase& C = cases[it.c];
+  const double* om = C.omega + (size_t)(it.k - 1) * C.ns;
+  double s = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < C.ns; t += gridDim.x * blockDim.x) s += om[t];
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+}
+
+__global__ void k_out_final(const DevCase* __restrict__ cases, const int* __restrict__ cids,
+                            const int* __restrict__ item_base, const double* __restrict__ partial) {
+  const DevCase& C = cases[cids[blockIdx.x]];
+  int tid = threadIdx.x;
+  double* out = C.out;
+  // circulation per level
+  if (tid < C.L) {
+    int base = item_base[blockIdx.x] + tid;
+    double s = 0.0;
+    for (int b = 0; b < kCircBlocks; b++) s += partial[base * kCircBlocks + b];
+    out[2 * C.nbody + tid] = s;
+  }
+  // forces per body: 2*delta * sum_f wsum_f * fb_f / dt
+  __shared__ double fxs[64], fys[64];
+  if (tid < 64) { fxs[tid] = 0.0; fys[tid] = 0.0; }
+  __syncthreads();
+  if (tid < C.nbody && tid < 64) {
+    int body = C.bmin + tid;
+    double sx = 0.0, sy = 0.0;
+    for (int p = 0; p < C.nb; p++)
+      if (C.bdyno[p] == body) {
+        sx += C.wsum[p] * (C.fb[p] / C.dt);
+        sy += C.wsum[C.nb + p] * (C.fb[C.nb + p] / C.dt);
+      }
+    out[tid] = sx * 2.0 * C.delta;
+    out[C.nbody + tid] = sy * 2.0 * C.delta;
+  }
+  // slip = max |regT(q_1) - motion|
+  __shared__ double mx[256];
+  double s = 0.0;
+  for (int f = tid; f < C.nf; f += blockDim.x) {
+    double d = fabs(regT_force(C, C.q, f) - C.motion[f]);
+    s = d > s ? d : s;
+  }
+  mx[tid] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (tid < w) mx[tid] = mx[tid] > mx[tid + w] ? mx[tid] : mx[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) out[2 * C.nbody + C.L] = mx[0];
+}
+
+__global__ void k_step_begin(const DevCase* __restrict__ cases, int ncases) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncases) *cases[c].itime += 1;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+void launch_lastbc(const DevCase* cases, const LevelItem* items, int nitems, int max_ring, cudaStream_t st) {
+  if (nitems == 0) return;
+  dim3 g((max_ring + 255) / 256, nitems);
+  k_lastbc<<<g, 256, 0, st>>>(cases, items);
+}
+void launch_rhs(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, int first, cudaStream_t st) {
+  if (nitems == 0) return;
+  dim3 g((max_ns + 255) / 256, nitems);
+  k_rhs<<<g, 256, 0, st>>>(cases, items, first);
+}
+void launch_coarsify(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, cudaStream_t st) {
+  if (nitems == 0) return;
+  dim3 g((max_ns / 4 + 255) / 256 + 1, nitems);
+  k_coarsify<<<g, 256, 0, st>>>(cases, items);
+}
+void launch_curl(const DevCase* cases, const LevelItem* items, int nitems, int max_nq, cudaStream_t st) {
+  if (nitems == 0) return;
+  dim3 g((max_nq + 255) / 256, nitems);
+  k_curl<<<g, 256, 0, st>>>(cases, items);
+}
+void launch_regrot(const DevCase* cases, const int* cids, int ncases, int max_ns, cudaStream_t st) {
+  if (ncases == 0) return;
+  dim3 g((max_ns + 255) / 256, ncases);
+  k_regrot<<<g, 256, 0, st>>>(cases, cids);
+}
+void launch_rhsf(const DevCase* cases, const int* cids, int ncases, int max_nf, cudaStream_t st) {
+  if (ncases == 0) return;
+  dim3 g((max_nf + 127) / 128, ncases);
+  k_rhsf<<<g, 128, 0, st>>>(cases, cids);
+}
+void launch_regT_out(const DevCase* cases, const int* cids, int ncases, int max_nf, double* const* outs,
+                     cudaStream_t st) {
+  if (ncases == 0) return;
+  dim3 g((max_nf + 127) / 128, ncases);
+  k_regT_out<<<g, 128, 0, st>>>(cases, cids, outs);
+}
+void launch_unit_fb(const DevCase* cases, const int* cids, const int* cols, int ncases, int max_nf,
+                    cudaStream_t st) {
+  if (ncases == 0) return;
+  dim3 g((max_nf + 127) / 128, ncases);
+  k_unit_fb<<<g, 128, 0, st>>>(cases, cids, cols);
+}
+void launch_outputs(const DevCase* cases, const LevelItem* items, int nitems, const int* cids, const int* item_base,
+                    int ncases, double* partial, cudaStream_t st) {
+  if (ncases == 0) return;
+  dim3 g(kCircBlocks, nitems);
+  k_out_partial<<<g, 256, 0, st>>>(cases, items, partial);
+  k_out_final<<<ncases, 256, 0, st>>>(cases, cids, item_base, partial);
+}
+void launch_step_begin(const DevCase* cases, int ncases, cudaStream_t st) {
+  k_step_begin<<<(ncases + 127) / 128, 128, 0, st>>>(cases, ncases);
+}
+
+}  // namespace ibfs

@@ -1,0 +1,218 @@
+"""ctypes binding of include/ibfs_capi.h (the B200 IBFS advance).
+
+This is the Python-side caller of the C-ABI, the same seam a Fortran driver
+binds through iso_c_binding. It loads the in-tree libibfs_b200.so and raises
+if it is missing -- there is no CPU fallback.
+
+Mirrors the reference's driver flow (src/main.f90:42-54): create (setup +
+setup_variables), optional restart/Cholesky load, then advance per step.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "libibfs_b200.so")
+
+OK, ERR_GRID, ERR_CHOL, ERR_CG_MAXITER, ERR_CUDA, ERR_IO, ERR_TIMEOUT, ERR_ARG, ERR_NOMEM = range(9)
+_ERRNAMES = {1: "IBFS_ERR_GRID", 2: "IBFS_ERR_CHOL", 3: "IBFS_ERR_CG_MAXITER", 4: "IBFS_ERR_CUDA",
+             5: "IBFS_ERR_IO", 6: "IBFS_ERR_TIMEOUT", 7: "IBFS_ERR_ARG", 8: "IBFS_ERR_NOMEM"}
+
+EXPORTS = [
+    "ibfs_create", "ibfs_batch_create", "ibfs_destroy", "ibfs_case_sizes", "ibfs_num_cases",
+    "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
+    "ibfs_advance", "ibfs_advance_n", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
+    "ibfs_last_timing", "ibfs_last_error",
+]
+
+
+class Params(ctypes.Structure):
+    """ibfs_params_c == namelist READ_PARAMETERS (parameters.f90:48-50)."""
+    _fields_ = [
+        ("istart", ctypes.c_int), ("istop", ctypes.c_int), ("isave", ctypes.c_int),
+        ("m", ctypes.c_int), ("n", ctypes.c_int),
+        ("dt", ctypes.c_double), ("re", ctypes.c_double), ("cgtol", ctypes.c_double),
+        ("cg_max_iter", ctypes.c_int), ("unif_flow", ctypes.c_int),
+        ("len", ctypes.c_double), ("offsetx", ctypes.c_double), ("offsety", ctypes.c_double),
+        ("mgridlev", ctypes.c_int), ("make_vortex", ctypes.c_int), ("stationary", ctypes.c_int),
+    ]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("precision", ctypes.c_int), ("cg_relative", ctypes.c_int), ("motion_kind", ctypes.c_int),
+        ("pitch_amp_deg", ctypes.c_double), ("pitch_freq", ctypes.c_double),
+        ("pivot_x", ctypes.c_double), ("pivot_y", ctypes.c_double), ("tile_cfg", ctypes.c_int),
+    ]
+
+
+class IbfsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+def lib():
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO):
+            raise FileNotFoundError(f"{SO} not built (run __graft_entry__.build() or make -C ibfs-if2d_b200)")
+        L = ctypes.CDLL(SO)
+        vp = ctypes.c_void_p
+        L.ibfs_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(Options), ctypes.c_int, _DP, _DP, _IP,
+                                  ctypes.POINTER(vp)]
+        L.ibfs_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(Options), _IP,
+                                        _DP, _DP, _IP, ctypes.POINTER(vp)]
+        L.ibfs_destroy.argtypes = [vp]
+        L.ibfs_case_sizes.argtypes = [vp, ctypes.c_int] + [_IP] * 6
+        L.ibfs_num_cases.argtypes = [vp]
+        L.ibfs_set_state.argtypes = [vp, ctypes.c_int, _DP, _DP, _DP, _DP, _DP]
+        L.ibfs_get_state.argtypes = [vp, ctypes.c_int, _DP, _DP, _DP, _DP, _DP]
+        L.ibfs_set_cholesky.argtypes = [vp, ctypes.c_int, _DP, _DP]
+        L.ibfs_get_cholesky.argtypes = [vp, ctypes.c_int, _DP, _DP]
+        L.ibfs_precompute.argtypes = [vp]
+        L.ibfs_advance.argtypes = [vp, _IP, _DP, _DP, _DP, _DP, _DP]
+        L.ibfs_advance_n.argtypes = [vp, ctypes.c_int, _DP]
+        L.ibfs_output_offset.argtypes = [vp, ctypes.c_int]
+        L.ibfs_output_stride.argtypes = [vp]
+        L.ibfs_apply_op.argtypes = [vp, ctypes.c_int, _DP, _DP]
+        L.ibfs_last_timing.argtypes = [vp, _DP]
+        L.ibfs_last_error.argtypes = [vp]
+        L.ibfs_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "float64 contiguous arrays only"
+    return a.ctypes.data_as(_DP)
+
+
+def make_params(m, n, dt, re, mgridlev, len_=4.0, offsetx=2.0, offsety=2.0, stationary=True,
+                unif_flow=True, cgtol=1e-7, cg_max_iter=3000, istart=0, istop=400, isave=25):
+    return Params(istart, istop, isave, m, n, dt, re, cgtol, cg_max_iter, int(unif_flow), len_,
+                  offsetx, offsety, mgridlev, 0, int(stationary))
+
+
+def make_options(precision=0, cg_relative=0, motion_kind=0, pitch_amp_deg=0.0, pitch_freq=0.0,
+                 pivot_x=0.0, pivot_y=0.0, tile_cfg=-1):
+    return Options(precision, cg_relative, motion_kind, pitch_amp_deg, pitch_freq, pivot_x, pivot_y,
+                   tile_cfg)
+
+
+class Solver:
+    """One handle: a single case (plain drop-in) or a batch of cases."""
+
+    def __init__(self, params, bodies, options=None):
+        """params: Params or list of Params; bodies: (xb, yb[, bdyno]) or list of those."""
+        L = lib()
+        if isinstance(params, Params):
+            params, bodies = [params], [bodies]
+            options = [options] if options is not None else None
+        n = len(params)
+        parr = (Params * n)(*params)
+        oarr = (Options * n)(*options) if options is not None else None
+        nb = np.array([len(b[0]) for b in bodies], dtype=np.int32)
+        xb = np.ascontiguousarray(np.concatenate([np.asarray(b[0], float) for b in bodies]))
+        yb = np.ascontiguousarray(np.concatenate([np.asarray(b[1], float) for b in bodies]))
+        bd = np.ascontiguousarray(np.concatenate(
+            [np.asarray(b[2] if len(b) > 2 else np.zeros(len(b[0])), dtype=np.int32) for b in bodies]))
+        h = ctypes.c_void_p()
+        rc = L.ibfs_batch_create(n, parr, oarr, nb.ctypes.data_as(_IP), _p(xb), _p(yb),
+                                 bd.ctypes.data_as(_IP), ctypes.byref(h))
+        if rc != 0:
+            raise IbfsError(rc, L.ibfs_last_error(None).decode())
+        self.h = h
+        self.ncases = n
+        self.sizes = []
+        for i in range(n):
+            v = [ctypes.c_int() for _ in range(6)]
+            L.ibfs_case_sizes(h, i, *[ctypes.byref(x) for x in v])
+            m_, n_, nlev, nq, nbp, nbody = [x.value for x in v]
+            self.sizes.append(dict(m=m_, n=n_, nlev=nlev, nq=nq, nb=nbp, nf=2 * nbp, nbody=nbody,
+                                   ns=(m_ - 1) * (n_ - 1)))
+        self.itime = ctypes.c_int(params[0].istart)
+        self.stride = L.ibfs_output_stride(h)
+
+    def close(self):
+        if getattr(self, "h", None) is not None:
+            lib().ibfs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise IbfsError(rc, lib().ibfs_last_error(self.h).decode())
+
+    def get_state(self, icase=0):
+        s = self.sizes[icase]
+        out = dict(omega=np.zeros(s["ns"] * s["nlev"]), fb=np.zeros(max(s["nf"], 1)),
+                   rhs_old=np.zeros(s["ns"] * s["nlev"]), q=np.zeros(s["nq"] * s["nlev"]),
+                   q0=np.zeros(s["nq"] * s["nlev"]))
+        self._check(lib().ibfs_get_state(self.h, icase, *[_p(out[k]) for k in
+                                                          ("omega", "fb", "rhs_old", "q", "q0")]))
+        return out
+
+    def set_state(self, icase=0, omega=None, fb=None, rhs_old=None, q=None, q0=None):
+        self._check(lib().ibfs_set_state(self.h, icase, _p(omega), _p(fb), _p(rhs_old), _p(q), _p(q0)))
+
+    def get_cholesky(self, icase=0):
+        nf = self.sizes[icase]["nf"]
+        cm, cv = np.zeros(nf * nf), np.zeros(nf)
+        self._check(lib().ibfs_get_cholesky(self.h, icase, _p(cm), _p(cv)))
+        return cm, cv
+
+    def set_cholesky(self, cm, cv, icase=0):
+        self._check(lib().ibfs_set_cholesky(self.h, icase, _p(np.ascontiguousarray(cm)),
+                                            _p(np.ascontiguousarray(cv))))
+
+    def precompute(self):
+        self._check(lib().ibfs_precompute(self.h))
+
+    def advance(self, body_vel=None):
+        s = self.sizes[0]
+        fx, fy = np.zeros(max(s["nbody"], 1)), np.zeros(max(s["nbody"], 1))
+        circ, slip = np.zeros(s["nlev"]), np.zeros(1)
+        bv = None if body_vel is None else np.ascontiguousarray(body_vel, dtype=np.float64)
+        self._check(lib().ibfs_advance(self.h, ctypes.byref(self.itime), _p(bv), _p(fx), _p(fy),
+                                       _p(circ), _p(slip)))
+        return dict(fx=fx, fy=fy, circ=circ, slip=float(slip[0]))
+
+    def advance_n(self, nsteps, want_hist=True):
+        hist = np.zeros(nsteps * self.stride) if want_hist else None
+        self._check(lib().ibfs_advance_n(self.h, nsteps, _p(hist)))
+        return hist.reshape(nsteps, self.stride) if want_hist else None
+
+    def outputs_of(self, hist_row, icase=0):
+        s = self.sizes[icase]
+        o = lib().ibfs_output_offset(self.h, icase)
+        nb = s["nbody"]
+        blk = hist_row[o:o + 2 * nb + s["nlev"] + 1]
+        return dict(fx=blk[:nb], fy=blk[nb:2 * nb], circ=blk[2 * nb:2 * nb + s["nlev"]],
+                    slip=blk[2 * nb + s["nlev"]])
+
+    def last_ms(self):
+        v = ctypes.c_double()
+        lib().ibfs_last_timing(self.h, ctypes.byref(v))
+        return v.value
+
+    def apply_op(self, op, x):
+        s = self.sizes[0]
+        nout = {0: s["ns"], 1: s["ns"], 2: s["ns"], 3: s["nf"], 4: s["nf"], 5: s["ns"]}[op]
+        out = np.zeros(nout)
+        self._check(lib().ibfs_apply_op(self.h, op, _p(np.ascontiguousarray(x, dtype=np.float64)), _p(out)))
+        return out

@@ -1,0 +1,144 @@
+/*
+ * ibfs_capi.h -- C-ABI of the B200-native IBFS per-timestep advance.
+ *
+ * Drop-in seam for the reference's in-process call CALL advance(it)
+ * (atchieu/ibfs-if2d src/main.f90:47-50) and its setup/output seams. Plain C
+ * types only (no CUDA or torch types): callable from Fortran iso_c_binding,
+ * C, C++ and ctypes. All arrays are host arrays in the reference's Fortran
+ * column-major layouts, 1-based semantics as documented per entry point:
+ *   omega, rhs_old  (m-1)*(n-1)*L   node (i,j), i=2..m fastest (variables.f90:46)
+ *   q, q0           Nq*L            u(i,j)=i+(j-1)(m+1), v(i,j)=(m+1)n+i+(j-1)m
+ *                                   (grid.f90:119-134), Nq=(m+1)n+(n+1)m
+ *   fb, body_vel    Nf=2*Nb         x-components then y-components (grid.f90:105-116)
+ *   cholmat, cholvec Nf*Nf, Nf      the ibfs.chd record (variables.f90:116-117)
+ * Every entry point returns an int status (IBFS_OK = 0). Calls on one handle
+ * are not reentrant; use one handle per host thread. Host arrays are never
+ * retained past a call.
+ */
+#ifndef IBFS_CAPI_H
+#define IBFS_CAPI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IBFS_OK 0
+#define IBFS_ERR_GRID 1        /* m or n not divisible by 4 (grid.f90:67-69)          */
+#define IBFS_ERR_CHOL 2        /* non-positive pivot, 'choldc failed' (operators.f90:784) */
+#define IBFS_ERR_CG_MAXITER 3  /* CG used cg_max_iter iterations (operators.f90:435-438) */
+#define IBFS_ERR_CUDA 4        /* CUDA runtime error; see ibfs_last_error              */
+#define IBFS_ERR_IO 5          /* restart / Cholesky file read or write failed         */
+#define IBFS_ERR_TIMEOUT 6     /* a bounded device wait gave up                        */
+#define IBFS_ERR_ARG 7         /* invalid argument (null pointer, case index, size)    */
+#define IBFS_ERR_NOMEM 8       /* device allocation failed                             */
+
+/* Namelist READ_PARAMETERS, field for field (parameters.f90:12-31, 48-50).
+ * Logical fields are ints (0 = .FALSE.). make_vortex is read but unused, as
+ * in the reference. */
+typedef struct {
+  int istart, istop, isave;
+  int m, n;
+  double dt, re, cgtol;
+  int cg_max_iter;
+  int unif_flow;
+  double len, offsetx, offsety;
+  int mgridlev;
+  int make_vortex;
+  int stationary;
+} ibfs_params_c;
+
+/* Options that the reference fixes in source; zero-initialised = reference
+ * behaviour, FP64. */
+typedef struct {
+  int precision;       /* 0: FP64 (plain method); 1: split-BF16 tensor-core transforms
+                          with one FP64 refinement sweep per solve                        */
+  int cg_relative;     /* 0: stop CG when r.r <= cgtol^2 (operators.f90:413-415);
+                          1: stop when ||r|| <= cgtol*||b||                             */
+  int motion_kind;     /* 0: body velocities from the caller per step (move_body,
+                          grid.f90:523-576); 1: rigid pitching about (pivot_x,pivot_y),
+                          alpha(t) = amp*sin(2 pi f t), points move, reg rebuilt        */
+  double pitch_amp_deg, pitch_freq, pivot_x, pivot_y;
+  int tile_cfg;        /* transform tile shape; -1 = chosen by the autotuner          */
+} ibfs_options_c;
+
+typedef struct ibfs_handle ibfs_handle;
+
+/* setup + setup_variables with istart=0 (grid.f90:44-139, variables.f90:28-77):
+ * grid indexing, level clamp (grid.f90:79-81), regularisation tables
+ * (setup_reg, grid.f90:142-230), spectral tables (setup_fft, myfft.f90:21-70),
+ * initial state (q0 = uniform flow when unif_flow). Body points as read from
+ * geom.inp (grid.f90:270-277). opt may be NULL. */
+int ibfs_create(const ibfs_params_c* p, const ibfs_options_c* opt, int nb, const double* xb,
+                const double* yb, const int* bdyno, ibfs_handle** out);
+
+/* Batched form: ncases independent cases of uneven sizes in one handle; one
+ * launch per kernel serves all cases. p, opt, nb have ncases entries; xb, yb,
+ * bdyno are the cases' body arrays concatenated. No reference counterpart
+ * (the reference runs one case per process). */
+int ibfs_batch_create(int ncases, const ibfs_params_c* p, const ibfs_options_c* opt, const int* nb,
+                      const double* xb, const double* yb, const int* bdyno, ibfs_handle** out);
+
+/* destroy_variables / destroy_grid (variables.f90:80-107). */
+int ibfs_destroy(ibfs_handle* h);
+
+/* Sizes after setup of case icase (mgridlev already clamped, grid.f90:81). */
+int ibfs_case_sizes(const ibfs_handle* h, int icase, int* m, int* n, int* nlev, int* nq, int* nb,
+                    int* nbody);
+int ibfs_num_cases(const ibfs_handle* h);
+
+/* read_variables / write_variables payload (variables.f90:141-175): the .var
+ * record omega, fb, rhs_old, q, q0 in that order. Any pointer may be NULL. */
+int ibfs_set_state(ibfs_handle* h, int icase, const double* omega, const double* fb,
+                   const double* rhs_old, const double* q, const double* q0);
+int ibfs_get_state(const ibfs_handle* h, int icase, double* omega, double* fb, double* rhs_old,
+                   double* q, double* q0);
+
+/* read_cholesky / write_cholesky payload (variables.f90:110-137): cholmat
+ * (upper triangle = A, strict lower = factor) and cholvec (diagonal). */
+int ibfs_set_cholesky(ibfs_handle* h, int icase, const double* cholmat, const double* cholvec);
+int ibfs_get_cholesky(const ibfs_handle* h, int icase, double* cholmat, double* cholvec);
+
+/* preprocess (operators.f90:29-59): A = [a_times(e_1) ... a_times(e_Nf)] built
+ * as one multi-right-hand-side pass on the GPU, then choldc on the GPU. Runs
+ * for every stationary case without a factor; ibfs_advance calls it at
+ * itime == 1 as the reference does. Returns IBFS_ERR_CHOL on a non-positive
+ * pivot. */
+int ibfs_precompute(ibfs_handle* h);
+
+/* advance (operators.f90:62-188) of a single-case handle. *itime is
+ * incremented as in the reference. body_vel: Nf body-point velocities in flow
+ * units (NULL = none); scaled by delta as move_body does (grid.f90:573-574).
+ * Outputs (any may be NULL): fx, fy per body (bodies minval..maxval(bdyno),
+ * write_force operators.f90:583-659, already divided by dt and times 2*delta),
+ * circ per level (write_circ :662-699), slip (write_slip :549-580). */
+int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx, double* fy,
+                 double* circ, double* slip);
+
+/* nsteps advances of every case, replayed from one captured CUDA graph per
+ * step. hist (may be NULL) receives, per step, per case, the output block
+ * [fx(nbody) fy(nbody) circ(L) slip]; ibfs_output_stride gives the per-case
+ * block length and ibfs_output_offset its offset within a step. */
+int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist);
+int ibfs_output_offset(const ibfs_handle* h, int icase);
+int ibfs_output_stride(const ibfs_handle* h);
+
+/* Individual operators of case 0 for verification (no reference counterpart
+ * as an entry point; each applies one reference function):
+ *   op 0 dst (myfft.f90:83-94)      in/out Ns
+ *   op 1 ctci (myfft.f90:97-109)    in/out Ns
+ *   op 2 ainv (myfft.f90:112-124)   in/out Ns
+ *   op 3 a_times (operators.f90:444-462)  in/out Nf
+ *   op 4 regT (operators.f90:531-546) in Nq, out Nf
+ *   op 5 reg + rot (operators.f90:513-528, 291-304) in Nf, out Ns          */
+int ibfs_apply_op(ibfs_handle* h, int op, const double* in, double* out);
+
+/* Device timing of the last ibfs_advance_n call: total milliseconds. */
+int ibfs_last_timing(const ibfs_handle* h, double* ms);
+
+/* Message of the last error on this handle (or of the last failed create). */
+const char* ibfs_last_error(const ibfs_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
