@@ -82,9 +82,10 @@ struct ibfs_handle {
   std::map<int, double*> sine;
   std::map<int, double*> costab;
   cudaStream_t st = nullptr;
-  std::vector<std::function<void()>> prog;
+  Prog prog;
   cudaGraphExec_t gexec = nullptr;
   bool graph_ok = false;
+  int graph_kernels = 0;  // kernel nodes in the captured step graph
   int* d_status = nullptr;
   int* d_itime = nullptr;
   double* d_out = nullptr;
@@ -218,7 +219,8 @@ static double* cos_table(ibfs_handle* h, int m) {
 // Step program construction
 struct ProgBuilder {
   ibfs_handle* h;
-  std::vector<std::function<void()>>& P;
+  Prog& P;
+  void add(std::function<void()> fn, int tag = TAG_STENCIL, double flops = 0.0) { P.push_back({fn, tag, flops}); }
   int cfg_for(const std::vector<GemmDesc>& ds) {
     if (h->tile_cfg >= 0) return h->tile_cfg;
     long tiles64 = 0;
@@ -233,7 +235,9 @@ struct ProgBuilder {
     GemmDesc* dd = dupload(h, ds);
     int nd = (int)ds.size();
     cudaStream_t st = h->st;
-    P.push_back([=]() { launch_gemm_f64(dd, nd, mt, cfg, dual, st); });
+    double fl = 0.0;
+    for (auto& d : ds) fl += 2.0 * d.M * (double)d.N * d.K * (dual ? 2 : 1);
+    add([=]() { launch_gemm_f64(dd, nd, mt, cfg, dual, st); }, TAG_GEMM_F64, fl);
   }
   const LevelItem* items(const std::vector<LevelItem>& v) { return dupload(h, v); }
   const int* ints(const std::vector<int>& v) { return dupload(h, v); }
@@ -277,7 +281,7 @@ static void build_vort2flux(ProgBuilder& B, const DevCase* dcases, const std::ve
     if (it.empty()) continue;
     const LevelItem* d = B.items(it);
     int ni = (int)it.size();
-    B.P.push_back([=]() { launch_coarsify(dcases, d, ni, mns, st); });
+    B.add([=]() { launch_coarsify(dcases, d, ni, mns, st); });
   }
   for (int t = 0; t < Lmax; t++) {
     std::vector<GemmDesc> r1, l1, r2, l2;
@@ -303,7 +307,7 @@ static void build_vort2flux(ProgBuilder& B, const DevCase* dcases, const std::ve
     for (int k = 1; k <= (curl_all ? cs[i].L : 1); k++) ci.push_back({ids[i], k});
   const LevelItem* d = B.items(ci);
   int ni = (int)ci.size();
-  B.P.push_back([=]() { launch_curl(dcases, d, ni, mnq, st); });
+  B.add([=]() { launch_curl(dcases, d, ni, mnq, st); });
 }
 
 // ainv(x) on level 1 (myfft.f90:112-124): x in c.vort, result stored (or
@@ -333,13 +337,13 @@ static void build_step_program(ibfs_handle* h) {
   int nc = (int)cs.size();
   int Lmax = h->max_L, mns = h->max_ns, mnf = h->max_nf, mring = h->max_ring;
   const int* d_ids = B.ints(ids);
-  h->prog.push_back([=]() { launch_step_begin(dcases, nc, st); });
+  B.add([=]() { launch_step_begin(dcases, nc, st); });
   // STEP 1 (operators.f90:97-134)
   std::vector<LevelItem> all;
   for (int i = 0; i < nc; i++) for (int k = 1; k <= cs[i].L; k++) all.push_back({i, k});
   const LevelItem* d_all = B.items(all);
   int nall = (int)all.size();
-  h->prog.push_back([=]() { launch_lastbc(dcases, d_all, nall, mring, st); });
+  B.add([=]() { launch_lastbc(dcases, d_all, nall, mring, st); });
   if (h->precision == 1) {
     build_precision_step1(h->prec, B.P, dcases, cs, st);
   } else {
@@ -362,7 +366,7 @@ static void build_step_program(ibfs_handle* h) {
       }
       const LevelItem* d = B.items(it);
       int ni = (int)it.size();
-      h->prog.push_back([=]() { launch_rhs(dcases, d, ni, mns, 0, st); });
+      B.add([=]() { launch_rhs(dcases, d, ni, mns, 0, st); });
       B.gemm(r1, false);
       B.gemm(l1, true);
       B.gemm(r2, false);
@@ -372,10 +376,10 @@ static void build_step_program(ibfs_handle* h) {
   // STEP 2 (operators.f90:142-171)
   if (h->precision == 1) build_precision_vort2flux(h->prec, B.P, dcases, cs, ids, false, st);
   else build_vort2flux(B, dcases, cs, ids, false);
-  h->prog.push_back([=]() { launch_rhsf(dcases, d_ids, nc, mnf, st); });
-  h->prog.push_back([=]() { launch_chol_solve(dcases, d_ids, nc, mnf, st); });
+  B.add([=]() { launch_rhsf(dcases, d_ids, nc, mnf, st); });
+  B.add([=]() { launch_chol_solve(dcases, d_ids, nc, mnf, st); }, TAG_CHOL);
   // STEP 3 (operators.f90:174)
-  h->prog.push_back([=]() { launch_regrot(dcases, d_ids, nc, mns, st); });
+  B.add([=]() { launch_regrot(dcases, d_ids, nc, mns, st); });
   if (h->precision == 1) build_precision_ainv(h->prec, B.P, dcases, cs, EPI_SUBTRACT, st);
   else build_ainv(B, cs, EPI_SUBTRACT);
   // STEP 4 (operators.f90:177)
@@ -387,7 +391,7 @@ static void build_step_program(ibfs_handle* h) {
   for (int i = 0; i < nc; i++) { base.push_back(acc); acc += cs[i].L; }
   const int* d_base = B.ints(base);
   double* part = h->d_partial;
-  h->prog.push_back([=]() { launch_outputs(dcases, d_all, nall, d_ids, d_base, nc, part, st); });
+  B.add([=]() { launch_outputs(dcases, d_all, nall, d_ids, d_base, nc, part, st); });
 }
 
 static int capture_graph(ibfs_handle* h) {
@@ -395,8 +399,17 @@ static int capture_graph(ibfs_handle* h) {
   h->graph_ok = false;
   cudaGraph_t g;
   if (cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return 0;
-  for (auto& f : h->prog) f();
+  for (auto& e : h->prog) e.fn();
   if (cudaStreamEndCapture(h->st, &g) != cudaSuccess) { cudaGetLastError(); return 0; }
+  size_t nn = 0;
+  cudaGraphGetNodes(g, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+  h->graph_kernels = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) h->graph_kernels++;
+  }
   if (cudaGraphInstantiate(&h->gexec, g, 0) == cudaSuccess) h->graph_ok = true;
   else cudaGetLastError();
   cudaGraphDestroy(g);
@@ -405,7 +418,7 @@ static int capture_graph(ibfs_handle* h) {
 
 static int run_step(ibfs_handle* h) {
   if (h->graph_ok) IBFS_CUDA_CHECK(cudaGraphLaunch(h->gexec, h->st));
-  else for (auto& f : h->prog) f();
+  else for (auto& e : h->prog) e.fn();
   IBFS_CUDA_CHECK(cudaGetLastError());
   return IBFS_OK;
 }
@@ -453,7 +466,7 @@ static int precompute(ibfs_handle* h) {
         cols[r] = j0 + r;
         outs[r] = c.chol + (size_t)(j0 + r) * c.nf;  // cholmat(:, j) = a_times(e_j)
       }
-      std::vector<std::function<void()>> P;
+      Prog P;
       ibfs_handle tmp;  // collects this chunk's uploads
       ProgBuilder B{&tmp, P};
       DevCase* dsh = dupload(&tmp, sh);
@@ -463,16 +476,16 @@ static int precompute(ibfs_handle* h) {
       cudaStream_t st = h->st;
       int mnf = c.nf, mns = c.ns;
       cudaMemsetAsync(pom, 0, sizeof(double) * nsL * nr, st);
-      P.push_back([=]() { launch_unit_fb(dsh, dids, dcols, nr, mnf, st); });
-      P.push_back([=]() { launch_regrot(dsh, dids, nr, mns, st); });
+      B.add([=]() { launch_unit_fb(dsh, dids, dcols, nr, mnf, st); });
+      B.add([=]() { launch_regrot(dsh, dids, nr, mns, st); });
       tmp.tile_cfg = h->tile_cfg;
       tmp.st = st;
       // A is always built in FP64 (the force system stays FP64 in every form)
       build_ainv(B, sh, EPI_STORE);
       build_vort2flux(B, dsh, sh, ids, false);
-      P.push_back([=]() { launch_regT_out(dsh, dids, nr, mnf, douts, st); });
+      B.add([=]() { launch_regT_out(dsh, dids, nr, mnf, douts, st); });
       for (auto& f : P) {
-        f();
+        f.fn();
         cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) { rc = fail_cuda(le, "preprocess launch"); break; }
       }
@@ -840,6 +853,34 @@ int ibfs_output_offset(const ibfs_handle* h, int icase) {
 }
 int ibfs_output_stride(const ibfs_handle* h) { return h ? h->out_stride : 0; }
 
+int ibfs_kernels_per_step(const ibfs_handle* h) { return h ? h->graph_kernels : -1; }
+
+int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops) {
+  if (!h || !ms || !launches || !flops) return IBFS_ERR_ARG;
+  size_t n = h->prog.size();
+  std::vector<cudaEvent_t> ev(n + 1);
+  for (auto& e : ev) IBFS_CUDA_CHECK(cudaEventCreate(&e));
+  for (int t = 0; t < TAG_NTAGS; t++) { ms[t] = 0.0; launches[t] = 0; flops[t] = 0.0; }
+  IBFS_CUDA_CHECK(cudaEventRecord(ev[0], h->st));
+  for (size_t i = 0; i < n; i++) {
+    h->prog[i].fn();
+    IBFS_CUDA_CHECK(cudaEventRecord(ev[i + 1], h->st));
+  }
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  IBFS_CUDA_CHECK(cudaGetLastError());
+  for (size_t i = 0; i < n; i++) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+    int tag = h->prog[i].tag;
+    ms[tag] += t;
+    launches[tag] += 1;
+    flops[tag] += h->prog[i].flops;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& c : h->cases) c.itime += 1;
+  return IBFS_OK;
+}
+
 int ibfs_last_timing(const ibfs_handle* h, double* ms) {
   if (!h || !ms) return IBFS_ERR_ARG;
   *ms = h->last_ms;
@@ -867,7 +908,7 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
   HostCase& hc = h->cases[0];
   DevCase c = hc.dc;
   cudaStream_t st = h->st;
-  std::vector<std::function<void()>> P;
+  Prog P;
   ibfs_handle tmp;
   tmp.st = st;
   tmp.tile_cfg = h->tile_cfg;
@@ -912,7 +953,7 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
     in_n = c.nf; out_n = c.nf;
     IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
     IBFS_CUDA_CHECK(cudaMemset(s.omega, 0, (size_t)c.L * ns * sizeof(double)));
-    P.push_back([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
+    B.add([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
     if (h->precision == 1) build_precision_ainv(h->prec, P, ds, sv, EPI_STORE, st);
     else build_ainv(B, sv, EPI_STORE);
     if (h->precision == 1) build_precision_vort2flux(h->prec, P, ds, sv, ids, false, st);
@@ -921,7 +962,7 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
     std::vector<double*> o1{s.wc};
     douts = dupload(&tmp, o1);
     int nf = c.nf;
-    P.push_back([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
+    B.add([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
     dout = s.wc;
   } else if (op == 4) {  // regT
     in_n = c.nq; out_n = c.nf;
@@ -929,19 +970,19 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
     std::vector<double*> o1{s.wc};
     double** douts = dupload(&tmp, o1);
     int nf = c.nf;
-    P.push_back([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
+    B.add([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
     dout = s.wc;
   } else if (op == 5) {  // rot(reg(f))
     in_n = c.nf; out_n = ns;
     IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
-    P.push_back([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
+    B.add([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
     dout = s.vort;
   } else {
     rc = fail(IBFS_ERR_ARG, "unknown op");
   }
   (void)in_n;
   if (rc == IBFS_OK) {
-    for (auto& f : P) f();
+    for (auto& f : P) f.fn();
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = fail_cuda(e, "apply_op");
     else if (cudaMemcpy(out, dout, out_n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)

@@ -1,8 +1,21 @@
 // ibfs_kernels.cuh -- launchers of the B200 IBFS kernels (host-callable).
 #pragma once
+#include <functional>
+#include <vector>
+
 #include "ibfs_common.cuh"
 
 namespace ibfs {
+
+// One launch (or a fixed pair of launches) of the step program, with its
+// class for profiling and its algorithmic flops.
+enum ProgTag { TAG_STENCIL = 0, TAG_GEMM_F64 = 1, TAG_GEMM_TC = 2, TAG_CHOL = 3, TAG_SPLIT = 4, TAG_NTAGS = 5 };
+struct ProgEntry {
+  std::function<void()> fn;
+  int tag;
+  double flops;
+};
+using Prog = std::vector<ProgEntry>;
 
 // Dense-GEMM sine transform (one half of a 2-D DST-I, myfft.f90:83-94):
 //   C(M x N) = A(M x K) * B(K x N), column-major, FP64, with fused prologue

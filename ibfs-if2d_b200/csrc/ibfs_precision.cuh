@@ -13,7 +13,6 @@ namespace ibfs {
 
 struct PrecisionPlan;
 using Alloc = std::function<void*(size_t)>;
-using Prog = std::vector<std::function<void()>>;
 
 int precision_init(PrecisionPlan*& pp, cudaStream_t st, const std::vector<DevCase>& cases, const DevCase* d_cases,
                    Alloc alloc);

@@ -23,7 +23,7 @@ EXPORTS = [
     "ibfs_create", "ibfs_batch_create", "ibfs_destroy", "ibfs_case_sizes", "ibfs_num_cases",
     "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
     "ibfs_advance", "ibfs_advance_n", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
-    "ibfs_last_timing", "ibfs_last_error",
+    "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_last_error",
 ]
 
 
@@ -84,6 +84,8 @@ def lib():
         L.ibfs_output_stride.argtypes = [vp]
         L.ibfs_apply_op.argtypes = [vp, ctypes.c_int, _DP, _DP]
         L.ibfs_last_timing.argtypes = [vp, _DP]
+        L.ibfs_kernels_per_step.argtypes = [vp]
+        L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
         L.ibfs_last_error.argtypes = [vp]
         L.ibfs_last_error.restype = ctypes.c_char_p
         _lib = L
@@ -195,6 +197,7 @@ class Solver:
     def advance_n(self, nsteps, want_hist=True):
         hist = np.zeros(nsteps * self.stride) if want_hist else None
         self._check(lib().ibfs_advance_n(self.h, nsteps, _p(hist)))
+        self.itime.value += nsteps
         return hist.reshape(nsteps, self.stride) if want_hist else None
 
     def outputs_of(self, hist_row, icase=0):
@@ -209,6 +212,18 @@ class Solver:
         v = ctypes.c_double()
         lib().ibfs_last_timing(self.h, ctypes.byref(v))
         return v.value
+
+    def kernels_per_step(self):
+        return lib().ibfs_kernels_per_step(self.h)
+
+    TAGS = ("stencil", "gemm_f64", "gemm_tc", "chol", "split")
+
+    def profile_step(self):
+        ms, fl = np.zeros(5), np.zeros(5)
+        la = np.zeros(5, dtype=np.int32)
+        self._check(lib().ibfs_profile_step(self.h, _p(ms), la.ctypes.data_as(_IP), _p(fl)))
+        self.itime.value += 1
+        return {t: dict(ms=float(ms[i]), launches=int(la[i]), flops=float(fl[i])) for i, t in enumerate(self.TAGS)}
 
     def apply_op(self, op, x):
         s = self.sizes[0]

@@ -135,6 +135,18 @@ int ibfs_apply_op(ibfs_handle* h, int op, const double* in, double* out);
 /* Device timing of the last ibfs_advance_n call: total milliseconds. */
 int ibfs_last_timing(const ibfs_handle* h, double* ms);
 
+/* Number of kernel launches in one captured step graph (no reference
+ * counterpart; reports the launch structure of the advance). */
+int ibfs_kernels_per_step(const ibfs_handle* h);
+
+/* Advances one step without the graph, with CUDA events around every launch
+ * on the handle's stream, and returns per launch class the summed device
+ * milliseconds, the launch count and the algorithmic flops (arrays of 5):
+ * 0 stencil / inter-level / IB, 1 FP64 transform GEMM, 2 tensor-core
+ * transform GEMM, 3 force solve, 4 split/refinement. No reference
+ * counterpart (measurement only). */
+int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops);
+
 /* Message of the last error on this handle (or of the last failed create). */
 const char* ibfs_last_error(const ibfs_handle* h);
 
