@@ -35,6 +35,8 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
+int set_error(int code, const char* msg) { return fail(code, msg); }
+
 // grid.f90:79: FLOOR(LOG(REAL(MIN(m,n)/2))/LOG(2.d0)) - 1 with single-precision LOG.
 static int nlevmax(int m, int n) {
   int mn = std::min(m, n) / 2;

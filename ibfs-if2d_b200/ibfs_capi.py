@@ -23,7 +23,8 @@ EXPORTS = [
     "ibfs_create", "ibfs_batch_create", "ibfs_destroy", "ibfs_case_sizes", "ibfs_num_cases",
     "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
     "ibfs_advance", "ibfs_advance_n", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
-    "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_last_error",
+    "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
+    "ibfs_last_error",
 ]
 
 
@@ -86,6 +87,8 @@ def lib():
         L.ibfs_last_timing.argtypes = [vp, _DP]
         L.ibfs_kernels_per_step.argtypes = [vp]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
+        L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p]
         L.ibfs_last_error.argtypes = [vp]
         L.ibfs_last_error.restype = ctypes.c_char_p
         _lib = L

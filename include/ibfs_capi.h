@@ -147,6 +147,22 @@ int ibfs_kernels_per_step(const ibfs_handle* h);
  * counterpart (measurement only). */
 int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops);
 
+/* 2-D DST-I (the reference's dst, myfft.f90:83-94) of a device field that
+ * allocates no device memory. No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc where they need a transform -- a driver
+ * whose memory pool owns all device memory, code running inside CUDA-graph
+ * stream capture, or a runtime that keeps the CUDA allocator off its solver
+ * thread. d_in, d_out: device pointers to (m-1)*(n-1) doubles in the Fortran
+ * node layout; stream: a cudaStream_t (NULL = default stream); the call is
+ * asynchronous on it. Limit: m-1, n-1 <= 511 (grids up to 512x512 cells),
+ * else IBFS_ERR_ARG. The intermediate product lives in one file-scope device
+ * array of 511*511 doubles (2.09 MB per GPU that loads the library, kept
+ * until exit), shared by all calls: calls that overlap on the GPU race and
+ * must be serialised by the caller. The first call on a device looks up that
+ * array's device address (with that device current); make the first call
+ * before any stream capture. Errors: ibfs_last_error(NULL). */
+int ibfs_dst2d_noalloc(const double* d_in, double* d_out, int m, int n, void* stream);
+
 /* Message of the last error on this handle (or of the last failed create). */
 const char* ibfs_last_error(const ibfs_handle* h);
 
