@@ -843,8 +843,11 @@ int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist) {
   if (hist)
     IBFS_CUDA_CHECK(cudaMemcpyAsync(hist, h->d_hist, sizeof(double) * (size_t)nsteps * h->out_stride,
                                     cudaMemcpyDeviceToHost, h->st));
+  int status = 0;
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
   IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
   cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  if (status & 2) return fail(IBFS_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM)");
   for (auto& c : h->cases) c.itime += nsteps;
   return IBFS_OK;
 }
