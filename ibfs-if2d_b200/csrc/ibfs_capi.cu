@@ -426,90 +426,103 @@ static int run_step(ibfs_handle* h) {
 }
 
 // ---------------------------------------------------------------------------
-// preprocess: a_times on unit vectors in chunks of shadow cases.
+// preprocess (operators.f90:29-59) for every stationary case lacking a factor:
+// the columns a_times(e_j) of all such cases are computed as "shadow cases"
+// (one per right-hand side, sharing the real case's grid tables, with private
+// scratch), packed from any mix of cases into chunks of a fixed memory budget
+// so that small cases share launches; then one CTA per case factors A.
 static int precompute(ibfs_handle* h) {
   std::vector<int> need;
   for (size_t i = 0; i < h->cases.size(); i++)
     if (h->cases[i].p.stationary && !h->cases[i].have_chol && h->cases[i].nf > 0) need.push_back((int)i);
   if (need.empty()) return IBFS_OK;
-  size_t budget = (size_t)4 << 30;
-  for (int ci : need) {
-    HostCase& hc = h->cases[ci];
-    const DevCase& c = hc.dc;
-    size_t per = sizeof(double) * ((size_t)(2 * c.L + 4) * c.ns + c.nq + c.nf);
-    int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)c.nf, budget / per));
-    // shadow pool
-    double *pom, *ps, *pw, *pq, *pf;
+  const size_t budget = (size_t)4 << 30;
+  auto per_rhs = [&](const DevCase& c) {
     size_t nsL = (size_t)c.L * c.ns;
-    if (cudaMalloc(&pom, sizeof(double) * nsL * chunk) != cudaSuccess ||
-        cudaMalloc(&ps, sizeof(double) * nsL * chunk) != cudaSuccess ||
-        cudaMalloc(&pw, sizeof(double) * 4 * c.ns * chunk) != cudaSuccess ||
-        cudaMalloc(&pq, sizeof(double) * c.nq * chunk) != cudaSuccess ||
-        cudaMalloc(&pf, sizeof(double) * c.nf * chunk) != cudaSuccess)
-      return fail(IBFS_ERR_NOMEM, "device allocation failed in preprocess");
-    std::vector<void*> tmp_allocs;
-    int rc = IBFS_OK;
-    for (int j0 = 0; j0 < c.nf && rc == IBFS_OK; j0 += chunk) {
-      int nr = std::min(chunk, c.nf - j0);
-      std::vector<DevCase> sh(nr, c);
-      std::vector<int> ids(nr), cols(nr);
-      std::vector<double*> outs(nr);
-      for (int r = 0; r < nr; r++) {
-        DevCase& s = sh[r];
-        s.omega = pom + nsL * r;
-        s.s = ps + nsL * r;
-        s.wa = pw + (size_t)4 * c.ns * r;
-        s.wb = s.wa + c.ns;
-        s.wc = s.wb + c.ns;
-        s.vort = s.wc + c.ns;
-        s.q = pq + (size_t)c.nq * r;
-        s.fb = pf + (size_t)c.nf * r;
-        ids[r] = r;
-        cols[r] = j0 + r;
-        outs[r] = c.chol + (size_t)(j0 + r) * c.nf;  // cholmat(:, j) = a_times(e_j)
-      }
-      Prog P;
-      ibfs_handle tmp;  // collects this chunk's uploads
-      ProgBuilder B{&tmp, P};
-      DevCase* dsh = dupload(&tmp, sh);
-      const int* dids = B.ints(ids);
-      const int* dcols = B.ints(cols);
-      double** douts = dupload(&tmp, outs);
-      cudaStream_t st = h->st;
-      int mnf = c.nf, mns = c.ns;
-      cudaMemsetAsync(pom, 0, sizeof(double) * nsL * nr, st);
-      B.add([=]() { launch_unit_fb(dsh, dids, dcols, nr, mnf, st); });
-      B.add([=]() { launch_regrot(dsh, dids, nr, mns, st); });
-      tmp.tile_cfg = h->tile_cfg;
-      tmp.st = st;
-      // A is always built in FP64 (the force system stays FP64 in every form)
-      build_ainv(B, sh, EPI_STORE);
-      build_vort2flux(B, dsh, sh, ids, false);
-      B.add([=]() { launch_regT_out(dsh, dids, nr, mnf, douts, st); });
-      for (auto& f : P) {
-        f.fn();
-        cudaError_t le = cudaGetLastError();
-        if (le != cudaSuccess) { rc = fail_cuda(le, "preprocess launch"); break; }
-      }
-      cudaError_t e = cudaStreamSynchronize(st);
-      if (rc == IBFS_OK && e != cudaSuccess) rc = fail_cuda(e, "preprocess a_times");
-      for (void* p : tmp.allocs) cudaFree(p);
-      tmp.allocs.clear();
+    size_t b = sizeof(double) * (2 * nsL + 4 * (size_t)c.ns + c.nq + c.nf);
+    return (b + 255) / 256 * 256;
+  };
+  char* pool = nullptr;
+  if (cudaMalloc(&pool, budget) != cudaSuccess) return fail(IBFS_ERR_NOMEM, "device allocation failed in preprocess");
+  struct Rhs { int ci, col; };
+  std::vector<Rhs> all;
+  for (int ci : need)
+    for (int j = 0; j < h->cases[ci].nf; j++) all.push_back({ci, j});
+  int rc = IBFS_OK;
+  size_t pos = 0;
+  while (pos < all.size() && rc == IBFS_OK) {
+    // pack right-hand sides until the pool is full
+    std::vector<DevCase> sh;
+    std::vector<int> cols;
+    std::vector<double*> outs;
+    size_t used = 0;
+    while (pos < all.size()) {
+      const DevCase& c = h->cases[all[pos].ci].dc;
+      size_t b = per_rhs(c);
+      if (used + b > budget && !sh.empty()) break;
+      if (b > budget) { rc = fail(IBFS_ERR_NOMEM, "one a_times column exceeds the preprocess pool"); break; }
+      DevCase s = c;
+      double* p = (double*)(pool + used);
+      size_t nsL = (size_t)c.L * c.ns;
+      s.omega = p; p += nsL;
+      s.s = p; p += nsL;
+      s.wa = p; p += c.ns;
+      s.wb = p; p += c.ns;
+      s.wc = p; p += c.ns;
+      s.vort = p; p += c.ns;
+      s.q = p; p += c.nq;
+      s.fb = p;
+      cudaMemsetAsync(s.omega, 0, sizeof(double) * nsL, h->st);
+      cols.push_back(all[pos].col);
+      outs.push_back(c.chol + (size_t)all[pos].col * c.nf);  // cholmat(:, j) = a_times(e_j)
+      sh.push_back(s);
+      used += b;
+      pos++;
     }
-    cudaFree(pom); cudaFree(ps); cudaFree(pw); cudaFree(pq); cudaFree(pf);
-    if (rc) return rc;
-    std::vector<int> one{ci};
-    int* dcid = dupload(h, one);
-    IBFS_CUDA_CHECK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
-    launch_chol_factor(h->d_cases, dcid, 1, h->d_status, h->st);
-    int status = 0;
-    IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-    IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
-    if (status) return fail(IBFS_ERR_CHOL, "choldc failed");
-    launch_chol_inverse(h->d_cases, dcid, 1, h->st);
-    IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
-    hc.have_chol = true;
+    if (rc) break;
+    int nr = (int)sh.size();
+    std::vector<int> ids(nr);
+    int mnf = 0, mns = 0;
+    for (int r = 0; r < nr; r++) { ids[r] = r; mnf = std::max(mnf, sh[r].nf); mns = std::max(mns, sh[r].ns); }
+    Prog P;
+    ibfs_handle tmp;  // collects this chunk's uploads
+    tmp.tile_cfg = h->tile_cfg;
+    tmp.st = h->st;
+    ProgBuilder B{&tmp, P};
+    DevCase* dsh = dupload(&tmp, sh);
+    const int* dids = B.ints(ids);
+    const int* dcols = B.ints(cols);
+    double** douts = dupload(&tmp, outs);
+    cudaStream_t st = h->st;
+    B.add([=]() { launch_unit_fb(dsh, dids, dcols, nr, mnf, st); });
+    B.add([=]() { launch_regrot(dsh, dids, nr, mns, st); });
+    // A is always built in FP64 (the force system stays FP64 in every form)
+    build_ainv(B, sh, EPI_STORE);
+    build_vort2flux(B, dsh, sh, ids, false);
+    B.add([=]() { launch_regT_out(dsh, dids, nr, mnf, douts, st); });
+    for (auto& f : P) {
+      f.fn();
+      cudaError_t le = cudaGetLastError();
+      if (le != cudaSuccess) { rc = fail_cuda(le, "preprocess launch"); break; }
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == IBFS_OK && e != cudaSuccess) rc = fail_cuda(e, "preprocess a_times");
+    for (void* p : tmp.allocs) cudaFree(p);
+    tmp.allocs.clear();
   }
+  cudaFree(pool);
+  if (rc) return rc;
+  int* dcid = dupload(h, need);
+  int nn = (int)need.size();
+  IBFS_CUDA_CHECK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->st));
+  launch_chol_factor(h->d_cases, dcid, nn, h->d_status, h->st);
+  int status = 0;
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  if (status) return fail(IBFS_ERR_CHOL, "choldc failed");
+  launch_chol_inverse(h->d_cases, dcid, nn, h->st);
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  for (int ci : need) h->cases[ci].have_chol = true;
   return IBFS_OK;
 }
 

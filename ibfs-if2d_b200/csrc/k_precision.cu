@@ -11,12 +11,14 @@
 //     x0 = S f S v        r = v - A x0 (FP64)        x = x0 + S f S r
 // which brings the ~1e-6 error of one split solve down to ~1e-12.
 //
-// GEMM kernel (k_gemm_tc): one CTA (128 threads) per 128x128 output tile;
-// K in blocks of 64; per K block six 16 KB operand tiles (A0..A2, B0..B2) are
-// staged into 128-byte-swizzled K-major shared memory with cp.async (two
-// stages, 192 KB); thread 0 issues 24 tcgen05.mma (M128 N128 K16, BF16 in,
-// FP32 accumulate) and commits to an mbarrier that frees the stage; the four
-// warps read the accumulator back with tcgen05.ld for the epilogue. All
+// GEMM kernel (k_gemm_tc<BN>): one CTA (128 threads) per 128 x BN output
+// tile, BN = 256 (K blocks of 32, 64-byte swizzle, 3 stages of 72 KB) or 128
+// for grids that 256 would pad (K blocks of 64, 128-byte swizzle, 2 stages of
+// 96 KB). Per K block six operand tiles (A0..A2, B0..B2) are brought into
+// swizzled K-major shared memory by TMA (issued by thread 0); thread 32 issues
+// the six slice products as tcgen05.mma (M128 N=BN K16, BF16 in, FP32
+// accumulate in TMEM) and commits to an mbarrier that frees the stage; the
+// four warps read the accumulator back with tcgen05.ld for the epilogue. All
 // mbarrier waits are bounded; a timeout sets an error flag and the CTA frees
 // its TMEM and returns.
 #include <cuda.h>
@@ -97,27 +99,34 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
-// K-major, 128-byte swizzle shared-memory matrix descriptor: 8-row groups
-// 1024 B apart (SBO), descriptor version 1, layout type 2 (SWIZZLE_128B).
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+// K-major swizzled shared-memory matrix descriptor for rows of BK BF16:
+// BK = 64 -> 128-byte rows, 128-byte swizzle (layout type 2), 8-row groups
+// 1024 B apart; BK = 32 -> 64-byte rows, 64-byte swizzle (layout type 4),
+// 8-row groups 512 B apart. LBO is unused for swizzled K-major; version 1.
+template <int BK>
+__device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)1 << 16;              // LBO (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;    // SBO
-  d |= (uint64_t)1 << 46;              // version
-  d |= (uint64_t)2 << 61;              // SWIZZLE_128B
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)((8 * BK * 2) >> 4) << 32;  // SBO
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)(BK == 64 ? 2 : 4) << 61;
   return d;
 }
 
-// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M=128, N=128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M=128, N=BN.
+template <int BN>
+constexpr uint32_t idesc_bf16() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
+}
 
+template <int BN>
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+      "l"(da), "l"(db), "r"(idesc_bf16<BN>()), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
       : "memory");
 }
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -154,13 +163,13 @@ enum TcEpi { TC_SPLIT_COL = 0, TC_SCALE_SPLIT_ROW = 1, TC_F64_STORE = 2, TC_F64_
 enum TcFactor { F_NONE = 0, F_LAMINV = 1, F_LAM1I_NORM = 2 };
 
 // One GEMM of one (case, level) item. Operands are 3-slice BF16 arrays
-// [slice][row][k] (k contiguous) described by TMA tensor maps (box 64 k x 128
-// rows, 128-byte swizzle); A rows are output rows, B rows output columns.
+// [slice][row][k] (k contiguous) described by TMA tensor maps (box 32 k x 128
+// rows, 64-byte swizzle); A rows are output rows, B rows output columns.
 struct __align__(64) TcDesc {
   CUtensorMap mapA;
   CUtensorMap mapB;
   int M, N, Kp;   // logical output extents; K padded to a multiple of 64
-  int tiles_m, tiles_n;
+  int tiles_m, tiles_n, bn;
   int epi, fkind;
   int ldcs, ldc;
   long long sC;
@@ -171,10 +180,16 @@ struct __align__(64) TcDesc {
   float nu, norm;     // F_LAM1I_NORM: 1/((1 + nu lam) norm); F_LAMINV: 1/(lam norm)
 };
 
-constexpr int kTcTile = 128, kTcBK = 64;
-constexpr int kTileBytes = kTcTile * kTcBK * 2;  // 16 KB
-constexpr int kStageBytes = 6 * kTileBytes;      // A0..A2, B0..B2
-constexpr int kTcSmem = 2 * kStageBytes + 1024 + 128;
+// Tile shapes: 128 x BN outputs, K blocks of BK, STAGES-deep operand ring.
+//   BN = 128: BK = 64 (128 B rows, 128 B swizzle), 2 stages of 96 KB
+//   BN = 256: BK = 32 (64 B rows, 64 B swizzle),   3 stages of 72 KB
+template <int BN> struct TcShape;
+template <> struct TcShape<128> { static constexpr int BK = 64, STAGES = 2; };
+template <> struct TcShape<256> { static constexpr int BK = 32, STAGES = 3; };
+template <int BN> constexpr int tc_a_bytes() { return 128 * TcShape<BN>::BK * 2; }
+template <int BN> constexpr int tc_b_bytes() { return BN * TcShape<BN>::BK * 2; }
+template <int BN> constexpr int tc_stage_bytes() { return 3 * tc_a_bytes<BN>() + 3 * tc_b_bytes<BN>(); }
+template <int BN> constexpr int tc_smem() { return TcShape<BN>::STAGES * tc_stage_bytes<BN>() + 1024 + 256; }
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
@@ -205,29 +220,32 @@ __device__ __forceinline__ void store8(bf16* dst, const bf16* v) {
   *reinterpret_cast<uint4*>(dst) = u;
 }
 
-// Warp-specialised: thread 0 issues the TMA loads, thread 32 the tcgen05.mma;
-// two stages of 96 KB; all four warps run the epilogue from TMEM.
+// Warp-specialised: thread 0 issues the TMA loads, thread 32 the tcgen05.mma
+// (six slice products per K block), all four warps run the epilogue from TMEM.
+template <int BN>
 __global__ void __launch_bounds__(128, 1) k_gemm_tc(const TcDesc* __restrict__ descs, int* __restrict__ status) {
+  constexpr int BK = TcShape<BN>::BK, S = TcShape<BN>::STAGES;
+  constexpr int AB = tc_a_bytes<BN>(), BB = tc_b_bytes<BN>(), SB = tc_stage_bytes<BN>();
   const TcDesc& d = descs[blockIdx.y];
   if ((int)blockIdx.x >= d.tiles_m * d.tiles_n) return;
-  const int m0 = (blockIdx.x % d.tiles_m) * kTcTile, n0 = (blockIdx.x / d.tiles_m) * kTcTile;
+  const int m0 = (blockIdx.x % d.tiles_m) * 128, n0 = (blockIdx.x / d.tiles_m) * BN;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* bars = (uint64_t*)(smem + 2 * kStageBytes);  // full[2], empty[2], done
-  uint32_t* tmem_slot = (uint32_t*)(smem + 2 * kStageBytes + 64);
+  uint64_t* bars = (uint64_t*)(smem + S * SB);  // full[S], empty[S], done
+  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + 8 * (2 * S + 1));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t sbase = smem_u32(smem);
-  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]), done = smem_u32(&bars[4]);
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[S]), done = smem_u32(&bars[2 * S]);
 
-  if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 128);
+  if (warp == 0) tmem_alloc(smem_u32(tmem_slot), BN);
   if (tid == 0) {
-    for (int b = 0; b < 5; b++) mbar_init(smem_u32(&bars[b]), 1);
+    for (int b = 0; b < 2 * S + 1; b++) mbar_init(smem_u32(&bars[b]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int nk = d.Kp / kTcBK;
+  const int nk = d.Kp / BK;
   bool to = false;
 
   if (tid == 0) {
@@ -235,33 +253,33 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const TcDesc* __restrict__ d
     asm volatile("prefetch.tensormap [%0];\n" ::"l"((uint64_t)&d.mapB) : "memory");
     int issued = 0;
     for (int kb = 0; kb < nk; kb++) {
-      const int s = kb & 1;
-      if (kb >= 2 && !mbar_spin(empty0 + 8 * s, ((kb >> 1) + 1) & 1)) { to = true; break; }
+      const int s = kb % S;
+      if (kb >= S && !mbar_spin(empty0 + 8 * s, ((kb / S) + 1) & 1)) { to = true; break; }
       const uint32_t fb = full0 + 8 * s;
-      mbar_expect_tx(fb, kStageBytes);
-      const uint32_t st = sbase + s * kStageBytes;
-      for (int t = 0; t < 3; t++) tma_load_3d(st + t * kTileBytes, &d.mapA, kb * kTcBK, m0, t, fb);
-      for (int t = 0; t < 3; t++) tma_load_3d(st + (3 + t) * kTileBytes, &d.mapB, kb * kTcBK, n0, t, fb);
+      mbar_expect_tx(fb, SB);
+      const uint32_t st = sbase + s * SB;
+      for (int t = 0; t < 3; t++) tma_load_3d(st + t * AB, &d.mapA, kb * BK, m0, t, fb);
+      for (int t = 0; t < 3; t++) tma_load_3d(st + 3 * AB + t * BB, &d.mapB, kb * BK, n0, t, fb);
       issued = kb + 1;
     }
     if (to) {  // let the copies already issued land before leaving
-      for (int kb = std::max(0, issued - 2); kb < issued; kb++) mbar_wait(full0 + 8 * (kb & 1), (kb >> 1) & 1);
+      for (int kb = issued > S ? issued - S : 0; kb < issued; kb++) mbar_wait(full0 + 8 * (kb % S), (kb / S) & 1);
     }
   } else if (tid == 32) {
     const int pa[6] = {0, 0, 1, 0, 1, 2};
     const int pb[6] = {0, 1, 0, 2, 1, 0};
     for (int kb = 0; kb < nk; kb++) {
-      const int s = kb & 1;
-      if (!mbar_spin(full0 + 8 * s, (kb >> 1) & 1)) { to = true; break; }
+      const int s = kb % S;
+      if (!mbar_spin(full0 + 8 * s, (kb / S) & 1)) { to = true; break; }
       tc_fence_after();
-      const uint32_t st = sbase + s * kStageBytes;
+      const uint32_t st = sbase + s * SB;
 #pragma unroll
       for (int p = 0; p < 6; p++) {
 #pragma unroll
-        for (int k16 = 0; k16 < 4; k16++) {
-          uint64_t da = smem_desc_sw128(st + pa[p] * kTileBytes + k16 * 32);
-          uint64_t db = smem_desc_sw128(st + (3 + pb[p]) * kTileBytes + k16 * 32);
-          umma_bf16(tmem, da, db, (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
+        for (int k16 = 0; k16 < BK / 16; k16++) {
+          uint64_t da = smem_desc_kmajor<BK>(st + pa[p] * AB + k16 * 32);
+          uint64_t db = smem_desc_kmajor<BK>(st + 3 * AB + pb[p] * BB + k16 * 32);
+          umma_bf16<BN>(tmem, da, db, (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
         }
       }
       umma_commit(empty0 + 8 * s);
@@ -274,7 +292,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const TcDesc* __restrict__ d
     if (tid == 0) atomicOr(status, 2);
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 128);
+    if (warp == 0) tmem_dealloc(tmem, BN);
     return;
   }
   tc_fence_after();
@@ -294,7 +312,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const TcDesc* __restrict__ d
   float* stg = reinterpret_cast<float*>(smem) + warp * (32 * 33);  // stage area is free now
   float lx = (epi == TC_SCALE_SPLIT_ROW && i < M) ? __ldg(&d.lamx[i]) : 0.f;
 #pragma unroll 1
-  for (int ch = 0; ch < kTcTile / 32; ch++) {
+  for (int ch = 0; ch < BN / 32; ch++) {
     float v[32];
     tmem_ld32(trow + ch * 32, v);
     const int jb = n0 + ch * 32;
@@ -351,7 +369,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const TcDesc* __restrict__ d
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 128);
+  if (warp == 0) tmem_dealloc(tmem, BN);
 }
 
 // ---------------------------------------------------------------------------
@@ -456,6 +474,7 @@ struct CaseBufs {
   CUtensorMap mapX, mapT, mapSm, mapSn;
   const float* lamx;
   const float* lamy;
+  int bn;  // output tile width of this case's GEMMs (128 or 256)
 };
 
 struct PrecisionPlan {
@@ -468,17 +487,27 @@ struct PrecisionPlan {
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
-// 3-D map over [slice][row][k] BF16 (k contiguous): box 64 x 128 x 1, 128 B swizzle.
-static bool make_map(CUtensorMap* map, const bf16* base, int ld, int rows, long long slice_stride) {
+static inline int rup(int x, int a) { return (x + a - 1) / a * a; }
+
+// 3-D map over [slice][row][k] BF16 (k contiguous): box bk x box_rows x 1,
+// swizzle matching the row length (bk=64: 128 B, bk=32: 64 B).
+static bool make_map(CUtensorMap* map, const bf16* base, int ld, int rows, long long slice_stride, int bk,
+                     int box_rows) {
   cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)rows, 3};
   cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)slice_stride * 2};
-  cuuint32_t box[3] = {64, 128, 1};
+  cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)box_rows, 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void*)base, dims, strides, box, es,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
+
+// Tile width for an output dimension N. Measured on B200 (256-case batch):
+// 128-wide tiles with 64-element K blocks (38.8 ms of GEMM per step) beat
+// 256-wide tiles with 32-element K blocks (42.2 ms), so 128 is used; the
+// 256-wide variant stays available to the tile autotuner.
+static int pick_bn(int N) { (void)N; return 128; }
 
 // lambda(i) = 2 - 2 cos(pi (i+1) / m) = 4 sin^2(pi (i+1) / 2m), free of cancellation.
 static float* lam_table(PrecisionPlan* pp, int m) {
@@ -495,12 +524,11 @@ static float* lam_table(PrecisionPlan* pp, int m) {
   return d;
 }
 
-static inline int rup(int x, int a) { return (x + a - 1) / a * a; }
 
 static std::pair<bf16*, long long> sine_slices(PrecisionPlan* pp, int m) {
   auto it = pp->sine.find(m);
   if (it != pp->sine.end()) return it->second;
-  int N = m - 1, R = rup(N, 128), ld = rup(N, 64);
+  int N = m - 1, R = rup(N, 256), ld = rup(N, 64);  // rows serve both GEMM roles
   long long sl = (long long)R * ld;
   std::vector<uint16_t> h((size_t)3 * sl, 0);
   for (int a = 0; a < N; a++)
@@ -535,7 +563,10 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   pp->alloc = alloc;
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<256>()) !=
+            cudaSuccess) {
       g_perr = "cannot raise shared memory limit for the tensor-core GEMM";
       return 4;
     }
@@ -553,7 +584,9 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   }
   for (auto& c : cases) {
     CaseBufs b{};
-    int Rm = rup(c.m - 1, 128), Rn = rup(c.n - 1, 128), Km = rup(c.m - 1, 64), Kn = rup(c.n - 1, 64);
+    b.bn = pick_bn(c.n - 1);
+    const int bk = b.bn == 256 ? 32 : 64;
+    int Rm = rup(c.m - 1, 128), Rn = rup(c.n - 1, b.bn), Km = rup(c.m - 1, 64), Kn = rup(c.n - 1, 64);
     b.sX = (long long)Rm * Kn;
     b.sT = (long long)Rn * Km;
     b.ldX = Kn;
@@ -570,8 +603,11 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
       g_perr = "device allocation failed for the split-precision buffers";
       return 8;
     }
-    if (!make_map(&b.mapX, b.Xs, Kn, Rm, b.sX) || !make_map(&b.mapT, b.Ts, Km, Rn, b.sT) ||
-        !make_map(&b.mapSm, b.Sm, Km, Rm, b.sSm) || !make_map(&b.mapSn, b.Sn, Kn, Rn, b.sSn)) {
+    const int Rs_m = rup(c.m - 1, 256), Rs_n = rup(c.n - 1, 256);
+    (void)Rs_m;
+    if (!make_map(&b.mapX, b.Xs, Kn, Rm, b.sX, bk, 128) || !make_map(&b.mapT, b.Ts, Km, Rn, b.sT, bk, b.bn) ||
+        !make_map(&b.mapSm, b.Sm, Km, rup(c.m - 1, 256), b.sSm, bk, 128) ||
+        !make_map(&b.mapSn, b.Sn, Kn, Rs_n, b.sSn, bk, b.bn)) {
       g_perr = "cuTensorMapEncodeTiled failed";
       return 4;
     }
@@ -600,22 +636,25 @@ static T* upload(PrecisionPlan* pp, const std::vector<T>& v) {
   return p;
 }
 
-static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& ds, cudaStream_t st) {
-  if (ds.empty()) return;
-  int mt = 0;
-  double fl = 0.0;
-  for (auto& d : ds) {
-    mt = std::max(mt, d.tiles_m * d.tiles_n);
-    fl += 2.0 * d.M * (double)d.N * (double)(d.epi == TC_SPLIT_COL ? d.N : d.M);  // algorithmic (unpadded) K
+static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all, cudaStream_t st) {
+  for (int bn : {128, 256}) {
+    std::vector<TcDesc> ds;
+    for (auto& d : all) if (d.bn == bn) ds.push_back(d);
+    if (ds.empty()) continue;
+    int mt = 0;
+    double fl = 0.0;
+    for (auto& d : ds) {
+      mt = std::max(mt, d.tiles_m * d.tiles_n);
+      fl += 2.0 * d.M * (double)d.N * (double)(d.epi == TC_SPLIT_COL ? d.N : d.M);  // algorithmic (unpadded) K
+    }
+    TcDesc* dd = upload(pp, ds);
+    int nd = (int)ds.size();
+    int* status = pp->status;
+    if (bn == 128)
+      P.push_back({[=]() { k_gemm_tc<128><<<dim3(mt, nd), 128, tc_smem<128>(), st>>>(dd, status); }, TAG_GEMM_TC, fl});
+    else
+      P.push_back({[=]() { k_gemm_tc<256><<<dim3(mt, nd), 128, tc_smem<256>(), st>>>(dd, status); }, TAG_GEMM_TC, fl});
   }
-  TcDesc* dd = upload(pp, ds);
-  int nd = (int)ds.size();
-  int* status = pp->status;
-  P.push_back({[=]() {
-                 dim3 g(mt, nd);
-                 k_gemm_tc<<<g, 128, kTcSmem, st>>>(dd, status);
-               },
-               TAG_GEMM_TC, fl});
 }
 
 static void add_prep(PrecisionPlan* pp, Prog& P, const std::vector<PrepDesc>& ds, cudaStream_t st) {
@@ -656,14 +695,14 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       }
       prep.push_back(pd);
       int M = c.m - 1, N = c.n - 1;
-      int tm = (M + 127) / 128, tn = (N + 127) / 128;
+      int tm = (M + 127) / 128, tn = (N + b.bn - 1) / b.bn;
       TcDesc R{};  // T = X * S_n
       R.mapA = b.mapX; R.mapB = b.mapSn;
-      R.M = M; R.N = N; R.Kp = rup(N, 64); R.tiles_m = tm; R.tiles_n = tn;
+      R.M = M; R.N = N; R.Kp = rup(N, 64); R.tiles_m = tm; R.tiles_n = tn; R.bn = b.bn;
       R.epi = TC_SPLIT_COL; R.Cs = b.Ts; R.sC = b.sT; R.ldcs = b.ldT;
       TcDesc L1{};  // U = f .* (S_m * T)
       L1.mapA = b.mapSm; L1.mapB = b.mapT;
-      L1.M = M; L1.N = N; L1.Kp = rup(M, 64); L1.tiles_m = tm; L1.tiles_n = tn;
+      L1.M = M; L1.N = N; L1.Kp = rup(M, 64); L1.tiles_m = tm; L1.tiles_n = tn; L1.bn = b.bn;
       L1.epi = TC_SCALE_SPLIT_ROW; L1.fkind = r.fkind; L1.Cs = b.Xs; L1.sC = b.sX; L1.ldcs = b.ldX;
       L1.lamx = b.lamx; L1.lamy = b.lamy; L1.norm = (float)c.norm;
       L1.nu = (float)(0.5 * c.dt / (c.delta * c.delta * std::pow(4.0, r.k - 1) * c.re));

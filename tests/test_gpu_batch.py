@@ -1,0 +1,50 @@
+"""Batched form: several independent cases of uneven size and level count in
+one handle (one launch per kernel for all of them) against the oracle run
+case by case, and against single-case handles."""
+import numpy as np
+import pytest
+
+import ibfs_capi as C
+import oracle as O
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+SMALL = [W.case(32, 3, 100.0, 0.01, "cylinder"), W.case(48, 2, 250.0, 0.008, "plate", aoa=20.0),
+         W.case(64, 3, 60.0, 0.006, "plate", aoa=35.0), W.case(32, 2, 400.0, 0.01, "plate", aoa=5.0, n=24)]
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 1e-8)])
+def test_batch_vs_oracle(precision, tol):
+    params, bodies, opts = W.solver_args(SMALL, C, precision)
+    g = C.Solver(params, bodies, opts)
+    steps = 6
+    hist = g.advance_n(steps)
+    for ic, c in enumerate(SMALL):
+        oc = O.Case(O.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"]), c["xb"], c["yb"])
+        fx = []
+        for _ in range(steps):
+            rc, o = oc.advance()
+            assert rc == 0
+            fx.append((o["fx"][0], o["fy"][0]))
+        fx = np.array(fx)
+        fg = np.array([[g.outputs_of(hist[s], ic)["fx"][0], g.outputs_of(hist[s], ic)["fy"][0]]
+                       for s in range(steps)])
+        cd = np.abs(fx[:, 0]).max()
+        assert np.abs(fg - fx).max() / cd < tol, ic
+        so, sg = oc.get_state(), g.get_state(ic)
+        assert rel(sg["omega"], so["omega"]) < tol, ic
+
+
+def test_batch_equals_single_handles():
+    params, bodies, opts = W.solver_args(SMALL, C, 0)
+    g = C.Solver(params, bodies, opts)
+    g.advance_n(4, want_hist=False)
+    for ic in range(len(SMALL)):
+        s = C.Solver(params[ic], bodies[ic], opts[ic])
+        s.advance_n(4, want_hist=False)
+        assert np.array_equal(s.get_state()["omega"], g.get_state(ic)["omega"]), ic
