@@ -84,10 +84,22 @@ struct ibfs_handle {
   std::map<int, double*> sine;
   std::map<int, double*> costab;
   cudaStream_t st = nullptr;
-  Prog prog;
-  cudaGraphExec_t gexec = nullptr;
+  Prog prog;                       // whole step (Cholesky handles) or the part before CG
+  Prog prog_iter, prog_iter50, prog_post;  // CG handles: one iteration, one with residual refresh, after CG
+  cudaGraphExec_t gexec = nullptr, gx_iter = nullptr, gx_iter50 = nullptr, gx_post = nullptr;
   bool graph_ok = false;
-  int graph_kernels = 0;  // kernel nodes in the captured step graph
+  int graph_kernels = 0;  // kernel nodes in the captured step graph(s), one CG iteration counted
+  bool cg = false;        // cases solve the force system by CG (stationary = .FALSE.)
+  int* d_cgit = nullptr;  // [ncases][2] iterations, active
+  // a_times shadows of the CG cases: input fb (x) or cg_d (d), private scratch
+  std::vector<DevCase> shx, shd;
+  std::vector<int> cg_ids;
+  DevCase *d_shx = nullptr, *d_shd = nullptr;
+  double* sh_omega = nullptr;
+  size_t sh_omega_bytes = 0;
+  int max_patch = 0, max_nb = 0;
+  std::vector<int> h_cgit;
+  int last_cg_iters = 0;
   int* d_status = nullptr;
   int* d_itime = nullptr;
   double* d_out = nullptr;
@@ -328,6 +340,32 @@ static void build_ainv(ProgBuilder& B, const std::vector<DevCase>& cs, int final
   B.gemm(l2, false);
 }
 
+// a_times (operators.f90:444-462) of every CG case in FP64 on its shadow:
+// vort(:,:,1) = ainv(rot(reg(x))), other levels zero; vort2flux(vel, vort, 1);
+// out = regT(vel). Input x is the shadow's fb (the case's fb for shx, cg_d
+// for shd).
+static void build_atimes_on(ProgBuilder& B, ibfs_handle* h, const DevCase* dsh, const std::vector<DevCase>& sh,
+                            double** d_out) {
+  cudaStream_t st = h->st;
+  double* om = h->sh_omega;
+  size_t ob = h->sh_omega_bytes;
+  B.add([=]() { cudaMemsetAsync(om, 0, ob, st); });
+  int n = (int)sh.size(), mns = 0, mnf = 0;
+  std::vector<int> ids(n);
+  for (int i = 0; i < n; i++) { ids[i] = i; mns = std::max(mns, sh[i].ns); mnf = std::max(mnf, sh[i].nf); }
+  const int* dids = B.ints(ids);
+  B.add([=]() { launch_regrot(dsh, dids, n, mns, st); }, TAG_CHOL);
+  build_ainv(B, sh, EPI_STORE);
+  build_vort2flux(B, dsh, sh, ids, false);
+  B.add([=]() { launch_regT_out(dsh, dids, n, mnf, d_out, st); }, TAG_CHOL);
+}
+static void build_atimes(ProgBuilder& B, ibfs_handle* h, double** d_out) {
+  build_atimes_on(B, h, h->d_shx, h->shx, d_out);
+}
+static void build_atimes_d(ProgBuilder& B, ibfs_handle* h, double** d_out) {
+  build_atimes_on(B, h, h->d_shd, h->shd, d_out);
+}
+
 static void build_step_program(ibfs_handle* h) {
   h->prog.clear();
   ProgBuilder B{h, h->prog};
@@ -340,6 +378,16 @@ static void build_step_program(ibfs_handle* h) {
   int Lmax = h->max_L, mns = h->max_ns, mnf = h->max_nf, mring = h->max_ring;
   const int* d_ids = B.ints(ids);
   B.add([=]() { launch_step_begin(dcases, nc, st); });
+  // move_body + setup_reg for moving bodies (operators.f90:142-144); step 1
+  // does not use the regularisation, so doing it first is equivalent
+  std::vector<int> mv;
+  for (int i = 0; i < nc; i++) if (cs[i].moving) mv.push_back(i);
+  if (!mv.empty()) {
+    const int* d_mv = B.ints(mv);
+    int nmv = (int)mv.size(), mnb = h->max_nb, mpatch = h->max_patch;
+    B.add([=]() { launch_move_body(dcases, d_mv, nmv, mnb, st); });
+    B.add([=]() { launch_setup_reg_moving(dcases, d_mv, nmv, mnf, mpatch, st); });
+  }
   // STEP 1 (operators.f90:97-134)
   std::vector<LevelItem> all;
   for (int i = 0; i < nc; i++) for (int k = 1; k <= cs[i].L; k++) all.push_back({i, k});
@@ -379,50 +427,129 @@ static void build_step_program(ibfs_handle* h) {
   if (h->precision == 1) build_precision_vort2flux(h->prec, B.P, dcases, cs, ids, false, st);
   else build_vort2flux(B, dcases, cs, ids, false);
   B.add([=]() { launch_rhsf(dcases, d_ids, nc, mnf, st); });
-  B.add([=]() { launch_chol_solve(dcases, d_ids, nc, mnf, st); }, TAG_CHOL);
+  std::vector<int> chol_ids;
+  for (int i = 0; i < nc; i++) if (h->cases[i].p.stationary) chol_ids.push_back(i);
+  if (!chol_ids.empty()) {
+    const int* d_ch = B.ints(chol_ids);
+    int nch = (int)chol_ids.size();
+    B.add([=]() { launch_chol_solve(dcases, d_ch, nch, mnf, st); }, TAG_CHOL);
+  }
+  h->prog_iter.clear();
+  h->prog_iter50.clear();
+  h->prog_post.clear();
+  if (h->cg) {
+    const int* d_cg = B.ints(h->cg_ids);
+    int ncg = (int)h->cg_ids.size();
+    std::vector<double*> oq, oq2;
+    for (int i : h->cg_ids) { oq.push_back(cs[i].cg_q); oq2.push_back(cs[i].cg_q2); }
+    double** d_oq = dupload(h, oq);
+    double** d_oq2 = dupload(h, oq2);
+    // r = b - A x, d = r (operators.f90:409-412)
+    build_atimes(B, h, d_oq);
+    B.add([=]() { launch_cg_start(dcases, d_cg, ncg, st); }, TAG_CHOL);
+    ProgBuilder Bi{h, h->prog_iter};
+    build_atimes_d(Bi, h, d_oq);
+    Bi.add([=]() { launch_cg_alpha(dcases, d_cg, ncg, 0, st); }, TAG_CHOL);
+    Bi.add([=]() { launch_cg_beta(dcases, d_cg, ncg, st); }, TAG_CHOL);
+    ProgBuilder B50{h, h->prog_iter50};
+    build_atimes_d(B50, h, d_oq);
+    B50.add([=]() { launch_cg_alpha(dcases, d_cg, ncg, 1, st); }, TAG_CHOL);
+    build_atimes(B50, h, d_oq2);
+    B50.add([=]() { launch_cg_resid(dcases, d_cg, ncg, st); }, TAG_CHOL);
+    B50.add([=]() { launch_cg_beta(dcases, d_cg, ncg, st); }, TAG_CHOL);
+  }
+  ProgBuilder Bp{h, h->cg ? h->prog_post : h->prog};
   // STEP 3 (operators.f90:174)
-  B.add([=]() { launch_regrot(dcases, d_ids, nc, mns, st); });
-  if (h->precision == 1) build_precision_ainv(h->prec, B.P, dcases, cs, EPI_SUBTRACT, st);
-  else build_ainv(B, cs, EPI_SUBTRACT);
+  Bp.add([=]() { launch_regrot(dcases, d_ids, nc, mns, st); });
+  if (h->precision == 1) build_precision_ainv(h->prec, Bp.P, dcases, cs, EPI_SUBTRACT, st);
+  else build_ainv(Bp, cs, EPI_SUBTRACT);
   // STEP 4 (operators.f90:177)
-  if (h->precision == 1) build_precision_vort2flux(h->prec, B.P, dcases, cs, ids, true, st);
-  else build_vort2flux(B, dcases, cs, ids, true);
+  if (h->precision == 1) build_precision_vort2flux(h->prec, Bp.P, dcases, cs, ids, true, st);
+  else build_vort2flux(Bp, dcases, cs, ids, true);
   // outputs (operators.f90:184-186)
   std::vector<int> base;
   int acc = 0;
   for (int i = 0; i < nc; i++) { base.push_back(acc); acc += cs[i].L; }
-  const int* d_base = B.ints(base);
+  const int* d_base = Bp.ints(base);
   double* part = h->d_partial;
-  B.add([=]() { launch_outputs(dcases, d_all, nall, d_ids, d_base, nc, part, st); });
+  Bp.add([=]() { launch_outputs(dcases, d_all, nall, d_ids, d_base, nc, part, st); });
 }
 
-static int capture_graph(ibfs_handle* h) {
-  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
-  h->graph_ok = false;
+static bool capture_one(ibfs_handle* h, Prog& P, cudaGraphExec_t* ex, int* kernels) {
+  if (*ex) { cudaGraphExecDestroy(*ex); *ex = nullptr; }
   cudaGraph_t g;
-  if (cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return 0;
-  for (auto& e : h->prog) e.fn();
-  if (cudaStreamEndCapture(h->st, &g) != cudaSuccess) { cudaGetLastError(); return 0; }
+  if (cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+  for (auto& e : P) e.fn();
+  if (cudaStreamEndCapture(h->st, &g) != cudaSuccess) { cudaGetLastError(); return false; }
   size_t nn = 0;
   cudaGraphGetNodes(g, nullptr, &nn);
   std::vector<cudaGraphNode_t> nodes(nn);
   if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
-  h->graph_kernels = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;
-    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) h->graph_kernels++;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) (*kernels)++;
   }
-  if (cudaGraphInstantiate(&h->gexec, g, 0) == cudaSuccess) h->graph_ok = true;
-  else cudaGetLastError();
+  bool ok = cudaGraphInstantiate(ex, g, 0) == cudaSuccess;
+  if (!ok) cudaGetLastError();
   cudaGraphDestroy(g);
+  return ok;
+}
+
+static int capture_graph(ibfs_handle* h) {
+  h->graph_kernels = 0;
+  h->graph_ok = capture_one(h, h->prog, &h->gexec, &h->graph_kernels);
+  if (h->cg) {
+    int k_iter = 0, k50 = 0;
+    h->graph_ok = h->graph_ok && capture_one(h, h->prog_iter, &h->gx_iter, &k_iter) &&
+                  capture_one(h, h->prog_iter50, &h->gx_iter50, &k50) &&
+                  capture_one(h, h->prog_post, &h->gx_post, &h->graph_kernels);
+    h->graph_kernels += k_iter;
+  }
   return 0;
 }
 
-static int run_step(ibfs_handle* h) {
-  if (h->graph_ok) IBFS_CUDA_CHECK(cudaGraphLaunch(h->gexec, h->st));
-  else for (auto& e : h->prog) e.fn();
+static int run_prog(ibfs_handle* h, Prog& P, cudaGraphExec_t ex) {
+  if (h->graph_ok && ex) IBFS_CUDA_CHECK(cudaGraphLaunch(ex, h->st));
+  else for (auto& e : P) e.fn();
   IBFS_CUDA_CHECK(cudaGetLastError());
   return IBFS_OK;
+}
+
+// One advance. CG handles replay the iteration graph in chunks of four and
+// read the per-case active flags between chunks (converged cases skip work
+// inside the CG kernels); returns IBFS_ERR_CG_MAXITER when a case used
+// cg_max_iter iterations (the reference warns and carries on, :435-438).
+static int run_step(ibfs_handle* h) {
+  int rc = run_prog(h, h->prog, h->gexec);
+  if (rc || !h->cg) return rc;
+  int maxit = 0;
+  for (auto& c : h->cases) maxit = std::max(maxit, c.p.cg_max_iter);
+  int nc = (int)h->cases.size();
+  int it = 0;
+  bool any = true, hit_max = false;
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(h->h_cgit.data(), h->d_cgit, sizeof(int) * 2 * nc, cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  any = false;
+  for (int c = 0; c < nc; c++) any = any || h->h_cgit[2 * c + 1] != 0;
+  while (any && it < maxit) {
+    for (int c = 0; c < 4 && it < maxit; c++) {
+      it++;
+      rc = (it % 50 == 0) ? run_prog(h, h->prog_iter50, h->gx_iter50) : run_prog(h, h->prog_iter, h->gx_iter);
+      if (rc) return rc;
+    }
+    IBFS_CUDA_CHECK(cudaMemcpyAsync(h->h_cgit.data(), h->d_cgit, sizeof(int) * 2 * nc, cudaMemcpyDeviceToHost, h->st));
+    IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+    any = false;
+    for (int c = 0; c < nc; c++) any = any || h->h_cgit[2 * c + 1] != 0;
+  }
+  h->last_cg_iters = 0;
+  for (int c = 0; c < nc; c++) {
+    h->last_cg_iters = std::max(h->last_cg_iters, h->h_cgit[2 * c]);
+    if (h->h_cgit[2 * c] >= h->cases[c].p.cg_max_iter) hit_max = true;
+  }
+  rc = run_prog(h, h->prog_post, h->gx_post);
+  if (rc) return rc;
+  return hit_max ? fail(IBFS_ERR_CG_MAXITER, "WARNING!! CJGR used max iterations!") : IBFS_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -602,6 +729,57 @@ static int setup_case(ibfs_handle* h, HostCase& c, const ibfs_params_c& p, const
   d.LinvT = dalloc<double>(h, (size_t)c.nf * c.nf);
   d.chol = dalloc<double>(h, (size_t)c.nf * c.nf + c.nf);
   if (!d.omega || !d.q || !d.s || !d.chol || !d.Sm || !d.Sn) return fail(IBFS_ERR_NOMEM, "device allocation failed");
+  d.offx = p.offsetx;
+  d.offy = p.offsety;
+  d.moving = c.o.motion_kind == 1 ? 1 : 0;
+  if (c.o.motion_kind != 0 && c.o.motion_kind != 1) return fail(IBFS_ERR_ARG, "unknown motion_kind");
+  if (d.moving) {
+    if (p.stationary) return fail(IBFS_ERR_ARG, "a moving body needs stationary = .FALSE. (CG force solve)");
+    const double pi = 3.1415926535897932384;
+    d.pitch_amp = c.o.pitch_amp_deg * pi / 180.0;
+    d.pitch_omega = 2.0 * pi * c.o.pitch_freq;
+    d.pivot_x = c.o.pivot_x;
+    d.pivot_y = c.o.pivot_y;
+    d.xb0 = dupload(h, c.xb);
+    d.yb0 = dupload(h, c.yb);
+    d.xb = dupload(h, c.xb);
+    d.yb = dupload(h, c.yb);
+    // patch of faces the body can reach: a disc around the pivot, 3 dx margin
+    double R = 0.0;
+    for (int k = 0; k < nb; k++)
+      R = std::max(R, std::hypot(c.xb[k] - d.pivot_x, c.yb[k] - d.pivot_y));
+    double mg = R + 3.0 * c.delta, dx = c.delta, h2 = 0.5 * dx;
+    auto lo = [&](double v, double off, int lim) { return std::max(1, (int)std::floor((v + off) / dx) + 1 - 1); };
+    auto hi = [&](double v, double off, int lim) { return std::min(lim, (int)std::ceil((v + off) / dx) + 1 + 1); };
+    d.pu_i0 = lo(d.pivot_x - mg, p.offsetx, c.m + 1);
+    d.pu_w = hi(d.pivot_x + mg, p.offsetx, c.m + 1) - d.pu_i0 + 1;
+    d.pu_j0 = lo(d.pivot_y - mg, p.offsety - h2, c.n);
+    d.pu_h = hi(d.pivot_y + mg, p.offsety - h2, c.n) - d.pu_j0 + 1;
+    d.pv_i0 = lo(d.pivot_x - mg, p.offsetx - h2, c.m);
+    d.pv_w = hi(d.pivot_x + mg, p.offsetx - h2, c.m) - d.pv_i0 + 1;
+    d.pv_j0 = lo(d.pivot_y - mg, p.offsety, c.n + 1);
+    d.pv_h = hi(d.pivot_y + mg, p.offsety, c.n + 1) - d.pv_j0 + 1;
+    int np = d.pu_w * d.pu_h + d.pv_w * d.pv_h;
+    d.pcnt = dalloc<int>(h, np);
+    d.pf = dalloc<int>(h, (size_t)np * kPatchCap);
+    d.pw = dalloc<double>(h, (size_t)np * kPatchCap);
+    d.tcnt = dalloc<int>(h, c.nf);
+    d.tface = dalloc<int>(h, (size_t)c.nf * 9);
+    d.tw = dalloc<double>(h, (size_t)c.nf * 9);
+    d.twsum = dalloc<double>(h, c.nf);
+    h->max_patch = std::max(h->max_patch, np);
+  }
+  h->max_nb = std::max(h->max_nb, nb);
+  if (!p.stationary) {
+    d.cg_r = dalloc<double>(h, c.nf);
+    d.cg_d = dalloc<double>(h, c.nf);
+    d.cg_q = dalloc<double>(h, c.nf);
+    d.cg_q2 = dalloc<double>(h, c.nf);
+    d.cg_sc = dalloc<double>(h, 4);
+    d.cgtol = p.cgtol;
+    d.cg_max_iter = p.cg_max_iter;
+    d.cg_rel = c.o.cg_relative;
+  }
   // initial state (variables.f90:55-64)
   if (p.unif_flow) {
     std::vector<double> q0(nqL, 0.0);
@@ -645,6 +823,43 @@ static int finish_create(ibfs_handle* h) {
     it0[i] = c.itime;
   }
   cudaMemcpy(h->d_itime, it0.data(), sizeof(int) * nc, cudaMemcpyHostToDevice);
+  // CG flags for every case; a_times shadows for the CG cases
+  h->d_cgit = dalloc<int>(h, 2 * nc);
+  h->h_cgit.assign(2 * nc, 0);
+  h->cg_ids.clear();
+  for (int i = 0; i < nc; i++) {
+    h->cases[i].dc.cg_it = h->d_cgit + 2 * i;
+    if (!h->cases[i].p.stationary) h->cg_ids.push_back(i);
+  }
+  h->cg = !h->cg_ids.empty();
+  if (h->cg) {
+    size_t om = 0, rest = 0;
+    for (int i : h->cg_ids) {
+      const DevCase& c = h->cases[i].dc;
+      om += (size_t)c.L * c.ns;
+      rest += (size_t)c.L * c.ns + c.nq + 4 * (size_t)c.ns;
+    }
+    h->sh_omega = dalloc<double>(h, om);
+    double* pr = dalloc<double>(h, rest);
+    if (!h->sh_omega || !pr) return fail(IBFS_ERR_NOMEM, "device allocation failed (CG scratch)");
+    h->sh_omega_bytes = om * sizeof(double);
+    double* po = h->sh_omega;
+    for (int i : h->cg_ids) {
+      DevCase s = h->cases[i].dc;
+      s.omega = po; po += (size_t)s.L * s.ns;
+      s.s = pr; pr += (size_t)s.L * s.ns;
+      s.q = pr; pr += s.nq;
+      s.wa = pr; pr += s.ns;
+      s.wb = pr; pr += s.ns;
+      s.wc = pr; pr += s.ns;
+      s.vort = pr; pr += s.ns;
+      h->shx.push_back(s);
+      s.fb = h->cases[i].dc.cg_d;
+      h->shd.push_back(s);
+    }
+    h->d_shx = dupload(h, h->shx);
+    h->d_shd = dupload(h, h->shd);
+  }
   std::vector<DevCase> dcs;
   for (auto& c : h->cases) dcs.push_back(c.dc);
   h->d_cases = dupload(h, dcs);
@@ -672,6 +887,9 @@ static void free_handle(ibfs_handle* h) {
   if (!h) return;
   if (h->st) cudaStreamSynchronize(h->st);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->gx_iter) cudaGraphExecDestroy(h->gx_iter);
+  if (h->gx_iter50) cudaGraphExecDestroy(h->gx_iter50);
+  if (h->gx_post) cudaGraphExecDestroy(h->gx_post);
   for (void* p : h->allocs) cudaFree(p);
   if (h->h_stage) cudaFreeHost(h->h_stage);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -872,6 +1090,8 @@ int ibfs_output_offset(const ibfs_handle* h, int icase) {
 int ibfs_output_stride(const ibfs_handle* h) { return h ? h->out_stride : 0; }
 
 int ibfs_kernels_per_step(const ibfs_handle* h) { return h ? h->graph_kernels : -1; }
+
+int ibfs_last_cg_iterations(const ibfs_handle* h) { return h ? h->last_cg_iters : -1; }
 
 int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops) {
   if (!h || !ms || !launches || !flops) return IBFS_ERR_ARG;

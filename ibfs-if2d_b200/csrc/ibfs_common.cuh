@@ -47,7 +47,33 @@ struct DevCase {
   double* out;  // fx[nbody], fy[nbody], circ[L], slip
   int* itime;   // device step counter
   int* status;  // device error flags
+
+  // moving body (rigid pitching about a pivot): positions, and per-step
+  // regularisation tables over a fixed patch of faces the body can reach
+  int moving;
+  double offx, offy;                                 // offsetx, offsety (grid origin)
+  double pitch_amp, pitch_omega, pivot_x, pivot_y;  // amplitude (rad), 2 pi f
+  const double *xb0, *yb0;  // positions at zero pitch
+  double *xb, *yb;          // current positions
+  int pu_i0, pu_j0, pu_w, pu_h;  // u-face patch: i in [pu_i0, pu_i0+pu_w), j in [pu_j0, pu_j0+pu_h)
+  int pv_i0, pv_j0, pv_w, pv_h;  // v-face patch
+  int* pcnt;                     // [patch faces] entries per face (u patch, then v patch)
+  int* pf;                       // [patch faces][kPatchCap] force index, ascending body point
+  double* pw;                    // [patch faces][kPatchCap] weight
+  int* tcnt;                     // [Nf] faces per force (<= 9)
+  int* tface;                    // [Nf][9] face index, ascending
+  double* tw;                    // [Nf][9] weight
+  double* twsum;                 // [Nf] sum of a force's weights
+
+  // conjugate gradient (operators.f90:393-441) on the force system
+  double *cg_r, *cg_d, *cg_q, *cg_q2;  // [Nf]
+  double* cg_sc;                       // delta_new, delta_old, eps, alpha
+  int* cg_it;                          // iterations, active flag
+  double cgtol;
+  int cg_max_iter, cg_rel;
 };
+
+constexpr int kPatchCap = 12;
 
 struct LevelItem {
   int c;  // case index

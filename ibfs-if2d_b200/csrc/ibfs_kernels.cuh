@@ -61,6 +61,15 @@ void launch_outputs(const DevCase* cases, const LevelItem* items, int nitems, co
                     int ncases, double* partial, cudaStream_t st);
 void launch_step_begin(const DevCase* cases, int ncases, cudaStream_t st);
 
+// Moving body and CG (grid.f90:523-576, 142-230; operators.f90:393-441).
+void launch_move_body(const DevCase* cases, const int* cids, int ncases, int max_nb, cudaStream_t st);
+void launch_setup_reg_moving(const DevCase* cases, const int* cids, int ncases, int max_nf, int max_patch,
+                             cudaStream_t st);
+void launch_cg_start(const DevCase* cases, const int* cids, int ncases, cudaStream_t st);
+void launch_cg_alpha(const DevCase* cases, const int* cids, int ncases, int recompute, cudaStream_t st);
+void launch_cg_resid(const DevCase* cases, const int* cids, int ncases, cudaStream_t st);
+void launch_cg_beta(const DevCase* cases, const int* cids, int ncases, cudaStream_t st);
+
 // Cholesky factor / inverse / solve (operators.f90:766-819).
 void launch_chol_factor(const DevCase* cases, const int* cids, int ncases, int* status, cudaStream_t st);
 void launch_chol_inverse(const DevCase* cases, const int* cids, int ncases, cudaStream_t st);

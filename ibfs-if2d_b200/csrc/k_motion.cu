@@ -1,0 +1,233 @@
+// k_motion.cu -- moving-body kernels: prescribed rigid pitching (move_body,
+// grid.f90:523-576), the per-step regularisation rebuild (setup_reg,
+// grid.f90:142-230) and the conjugate-gradient force solve (cjgr,
+// operators.f90:393-441). All FP64.
+//
+// setup_reg for a moving body is rebuilt on the device every step into two
+// fixed-capacity tables: per force, its <= 3x3 faces in ascending face index
+// (the order of regT's scatter loop); per face of a fixed patch around the
+// body's reach, its body points in ascending order (the order of reg's sum).
+// Both use the reference's box test |x-xb| < 1.5 dx and the Roma-Peskin-Berger
+// 3-point kernel.
+#include "ibfs_common.cuh"
+#include "ibfs_kernels.cuh"
+
+namespace ibfs {
+
+// grid.f90:233-249.
+__device__ __forceinline__ double deltafnc_d(double r, double r0, double dr) {
+  double d = fabs(r - r0);
+  if (d <= 0.5 * dr) {
+    double t = (r - r0) / dr;
+    return (1.0 + sqrt(-3.0 * t * t + 1.0)) / (3.0 * dr);
+  } else if (d <= 1.5 * dr) {
+    double a = fabs((r - r0) / dr);
+    double u = 1.0 - a;
+    return (5.0 - 3.0 * a - sqrt(-3.0 * u * u + 1.0)) / (6.0 * dr);
+  }
+  return 0.0;
+}
+
+// Rigid pitching about (pivot_x, pivot_y): the body is the zero-pitch shape
+// turned by -alpha(t) (the sign convention of line(), grid.f90:442), with
+// alpha(t) = amp sin(omega t), t = itime dt; body velocity = rotation rate x r.
+__global__ void k_move_body(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= C.nb) return;
+  double t = C.dt * (double)(*C.itime);
+  double al = C.pitch_amp * sin(C.pitch_omega * t);
+  double ald = C.pitch_amp * C.pitch_omega * cos(C.pitch_omega * t);
+  double th = -al, thd = -ald;
+  double c = cos(th), s = sin(th);
+  double rx = C.xb0[k] - C.pivot_x, ry = C.yb0[k] - C.pivot_y;
+  double x = C.pivot_x + c * rx - s * ry;
+  double y = C.pivot_y + s * rx + c * ry;
+  C.xb[k] = x;
+  C.yb[k] = y;
+  C.bvel[k] = -thd * (y - C.pivot_y);
+  C.bvel[C.nb + k] = thd * (x - C.pivot_x);
+}
+
+// Per-force table: u faces at (dx(i-1)-ox, dx(j-1)-oy+dx/2), v faces at
+// (dx(i-1)-ox+dx/2, dx(j-1)-oy); candidates scanned j-major for ascending
+// face index.
+__global__ void k_setup_reg_force(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  const double ox = C.offx, oy = C.offy;
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= C.nf) return;
+  int m = C.m, n = C.n, nb = C.nb;
+  bool vcomp = f >= nb;
+  int k = vcomp ? f - nb : f;
+  double dx = C.delta, d2 = 0.5 * dx, sup = 3.0 * d2;
+  double xk = C.xb[k], yk = C.yb[k];
+  double sx = vcomp ? d2 : 0.0, sy = vcomp ? 0.0 : d2;
+  int ic = (int)floor((xk + ox - sx) / dx) + 1, jc = (int)floor((yk + oy - sy) / dx) + 1;
+  int imax = vcomp ? m : m + 1, jmax = vcomp ? n + 1 : n;
+  int cnt = 0;
+  double ws = 0.0;
+  for (int j = jc - 2; j <= jc + 2; j++) {
+    if (j < 1 || j > jmax) continue;
+    for (int i = ic - 2; i <= ic + 2; i++) {
+      if (i < 1 || i > imax) continue;
+      double x = dx * (double)(i - 1) - ox + sx;
+      double y = dx * (double)(j - 1) - oy + sy;
+      if (fabs(x - xk) < sup && fabs(y - yk) < sup && cnt < 9) {
+        double w = (dx * dx) * deltafnc_d(x, xk, dx) * deltafnc_d(y, yk, dx);
+        C.tface[f * 9 + cnt] = vcomp ? (m + 1) * n + (i - 1) + (j - 1) * m : (i - 1) + (j - 1) * (m + 1);
+        C.tw[f * 9 + cnt] = w;
+        ws += w;
+        cnt++;
+      }
+    }
+  }
+  C.tcnt[f] = cnt;
+  C.twsum[f] = ws;
+}
+
+// Per-face table over the patch: body points in ascending order.
+__global__ void k_setup_reg_patch(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  const double ox = C.offx, oy = C.offy;
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int nu_p = C.pu_w * C.pu_h, np = nu_p + C.pv_w * C.pv_h;
+  if (p >= np) return;
+  double dx = C.delta, d2 = 0.5 * dx, sup = 3.0 * d2;
+  bool vcomp = p >= nu_p;
+  int i, j;
+  if (!vcomp) { i = p % C.pu_w + C.pu_i0; j = p / C.pu_w + C.pu_j0; }
+  else { int q = p - nu_p; i = q % C.pv_w + C.pv_i0; j = q / C.pv_w + C.pv_j0; }
+  double x = dx * (double)(i - 1) - ox + (vcomp ? d2 : 0.0);
+  double y = dx * (double)(j - 1) - oy + (vcomp ? 0.0 : d2);
+  int cnt = 0;
+  for (int k = 0; k < C.nb; k++) {
+    double xk = C.xb[k], yk = C.yb[k];
+    if (fabs(x - xk) < sup && fabs(y - yk) < sup) {
+      if (cnt < kPatchCap) {
+        C.pf[p * kPatchCap + cnt] = vcomp ? C.nb + k : k;
+        C.pw[p * kPatchCap + cnt] = (dx * dx) * deltafnc_d(x, xk, dx) * deltafnc_d(y, yk, dx);
+      } else {
+        atomicOr(C.status, 4);  // patch capacity exceeded
+      }
+      cnt++;
+    }
+  }
+  C.pcnt[p] = cnt < kPatchCap ? cnt : kPatchCap;
+}
+
+// --------------------------------------------------------------------------
+// CG (operators.f90:393-441), one CTA per case, FP64 reductions in a fixed
+// order (block tree). Scalars: sc[0] delta_new, sc[1] delta_old, sc[2] eps,
+// sc[3] alpha; it[0] iterations, it[1] active.
+__device__ double block_dot(const double* a, const double* b, int n, double* red) {
+  double s = 0.0;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) s = fma(a[t], b[t], s);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// r = b - A x (A x in cg_q), d = r, delta_new = r.r, eps, active.
+__global__ void k_cg_start(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.x]];
+  __shared__ double red[256];
+  int nf = C.nf;
+  for (int t = threadIdx.x; t < nf; t += blockDim.x) {
+    double r = C.rhsf[t] - C.cg_q[t];
+    C.cg_r[t] = r;
+    C.cg_d[t] = r;
+  }
+  __syncthreads();
+  double dn = block_dot(C.cg_r, C.cg_r, nf, red);
+  double eps = C.cgtol * C.cgtol;
+  if (C.cg_rel) eps = eps * block_dot(C.rhsf, C.rhsf, nf, red);
+  if (threadIdx.x == 0) {
+    C.cg_sc[0] = dn;
+    C.cg_sc[2] = eps;
+    C.cg_it[0] = 0;
+    C.cg_it[1] = (C.cg_max_iter > 0 && dn > eps) ? 1 : 0;
+  }
+}
+
+// alpha = delta_new / d.q ; x += alpha d ; r -= alpha q unless it is recomputed.
+__global__ void k_cg_alpha(const DevCase* __restrict__ cases, const int* __restrict__ cids, int recompute) {
+  const DevCase& C = cases[cids[blockIdx.x]];
+  if (!C.cg_it[1]) return;
+  __shared__ double red[256];
+  int nf = C.nf;
+  double dq = block_dot(C.cg_d, C.cg_q, nf, red);
+  double alpha = C.cg_sc[0] / dq;
+  for (int t = threadIdx.x; t < nf; t += blockDim.x) {
+    C.fb[t] = C.fb[t] + alpha * C.cg_d[t];
+    if (!recompute) C.cg_r[t] = C.cg_r[t] - alpha * C.cg_q[t];
+  }
+  if (threadIdx.x == 0) C.cg_sc[3] = alpha;
+}
+
+// r = b - A x with A x in cg_q2 (every 50th iteration, operators.f90:421-422).
+__global__ void k_cg_resid(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.x]];
+  if (!C.cg_it[1]) return;
+  for (int t = threadIdx.x; t < C.nf; t += blockDim.x) C.cg_r[t] = C.rhsf[t] - C.cg_q2[t];
+}
+
+// delta_old = delta_new; delta_new = r.r; d = r + beta d; iter++; active.
+__global__ void k_cg_beta(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.x]];
+  if (!C.cg_it[1]) return;
+  __shared__ double red[256];
+  int nf = C.nf;
+  double dn = block_dot(C.cg_r, C.cg_r, nf, red);
+  double beta = dn / C.cg_sc[0];
+  for (int t = threadIdx.x; t < nf; t += blockDim.x) C.cg_d[t] = C.cg_r[t] + beta * C.cg_d[t];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    C.cg_sc[1] = C.cg_sc[0];
+    C.cg_sc[0] = dn;
+    int it = C.cg_it[0] + 1;
+    C.cg_it[0] = it;
+    C.cg_it[1] = (it < C.cg_max_iter && dn > C.cg_sc[2]) ? 1 : 0;
+  }
+}
+
+// Copy a face field (the a_times input vector) into a shadow's fb.
+__global__ void k_copy_vec(double* const* __restrict__ dst, const double* const* __restrict__ src,
+                           const int* __restrict__ n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n[blockIdx.y]) dst[blockIdx.y][i] = src[blockIdx.y][i];
+}
+
+void launch_move_body(const DevCase* cases, const int* cids, int ncases, int max_nb, cudaStream_t st) {
+  if (ncases) k_move_body<<<dim3((max_nb + 127) / 128, ncases), 128, 0, st>>>(cases, cids);
+}
+void launch_setup_reg_moving(const DevCase* cases, const int* cids, int ncases, int max_nf, int max_patch,
+                             cudaStream_t st) {
+  if (!ncases) return;
+  k_setup_reg_force<<<dim3((max_nf + 127) / 128, ncases), 128, 0, st>>>(cases, cids);
+  k_setup_reg_patch<<<dim3((max_patch + 127) / 128, ncases), 128, 0, st>>>(cases, cids);
+}
+void launch_cg_start(const DevCase* cases, const int* cids, int ncases, cudaStream_t st) {
+  if (ncases) k_cg_start<<<ncases, 256, 0, st>>>(cases, cids);
+}
+void launch_cg_alpha(const DevCase* cases, const int* cids, int ncases, int recompute, cudaStream_t st) {
+  if (ncases) k_cg_alpha<<<ncases, 256, 0, st>>>(cases, cids, recompute);
+}
+void launch_cg_resid(const DevCase* cases, const int* cids, int ncases, cudaStream_t st) {
+  if (ncases) k_cg_resid<<<ncases, 256, 0, st>>>(cases, cids);
+}
+void launch_cg_beta(const DevCase* cases, const int* cids, int ncases, cudaStream_t st) {
+  if (ncases) k_cg_beta<<<ncases, 256, 0, st>>>(cases, cids);
+}
+void launch_copy_vec(double* const* dst, const double* const* src, const int* n, int nvec, int max_n,
+                     cudaStream_t st) {
+  if (nvec) k_copy_vec<<<dim3((max_n + 127) / 128, nvec), 128, 0, st>>>(dst, src, n);
+}
+
+}  // namespace ibfs

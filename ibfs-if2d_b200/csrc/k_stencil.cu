@@ -162,6 +162,22 @@ __global__ void k_curl(const DevCase* __restrict__ cases, const LevelItem* __res
 // rot :291-304). reg is gathered per face from the CSR-by-face table whose
 // entries keep the reference's smear order.
 __device__ __forceinline__ double reg_face(const DevCase& C, const double* __restrict__ f, int face) {
+  if (C.moving) {  // patch tables rebuilt every step
+    int m = C.m, nu = (m + 1) * C.n, pidx;
+    if (face < nu) {
+      int i = face % (m + 1) + 1 - C.pu_i0, j = face / (m + 1) + 1 - C.pu_j0;
+      if (i < 0 || j < 0 || i >= C.pu_w || j >= C.pu_h) return 0.0;
+      pidx = i + j * C.pu_w;
+    } else {
+      int fv = face - nu;
+      int i = fv % m + 1 - C.pv_i0, j = fv / m + 1 - C.pv_j0;
+      if (i < 0 || j < 0 || i >= C.pv_w || j >= C.pv_h) return 0.0;
+      pidx = C.pu_w * C.pu_h + i + j * C.pv_w;
+    }
+    double h = 0.0;
+    for (int p = 0; p < C.pcnt[pidx]; p++) h = h + C.pw[pidx * kPatchCap + p] * f[C.pf[pidx * kPatchCap + p]];
+    return h;
+  }
   int p0 = C.face_ptr[face], p1 = C.face_ptr[face + 1];
   double h = 0.0;
   for (int p = p0; p < p1; p++) h = h + C.face_w[p] * f[C.face_f[p]];
@@ -183,6 +199,11 @@ __global__ void k_regrot(const DevCase* __restrict__ cases, const int* __restric
 // regT (operators.f90:531-546) of one face field, gathered per force in the
 // reference's scatter order (ascending face index).
 __device__ __forceinline__ double regT_force(const DevCase& C, const double* __restrict__ h, int f) {
+  if (C.moving) {
+    double s = 0.0;
+    for (int p = 0; p < C.tcnt[f]; p++) s = s + C.tw[f * 9 + p] * h[C.tface[f * 9 + p]];
+    return s;
+  }
   int p0 = C.force_ptr[f], p1 = C.force_ptr[f + 1];
   double s = 0.0;
   for (int p = p0; p < p1; p++) s = s + C.force_w[p] * h[C.force_face[p]];
@@ -260,8 +281,9 @@ __global__ void k_out_final(const DevCase* __restrict__ cases, const int* __rest
     double sx = 0.0, sy = 0.0;
     for (int p = 0; p < C.nb; p++)
       if (C.bdyno[p] == body) {
-        sx += C.wsum[p] * (C.fb[p] / C.dt);
-        sy += C.wsum[C.nb + p] * (C.fb[C.nb + p] / C.dt);
+        const double* ws = C.moving ? C.twsum : C.wsum;
+        sx += ws[p] * (C.fb[p] / C.dt);
+        sy += ws[C.nb + p] * (C.fb[C.nb + p] / C.dt);
       }
     out[tid] = sx * 2.0 * C.delta;
     out[C.nbody + tid] = sy * 2.0 * C.delta;

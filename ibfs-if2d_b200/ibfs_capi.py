@@ -24,6 +24,7 @@ EXPORTS = [
     "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
     "ibfs_advance", "ibfs_advance_n", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
+    "ibfs_last_cg_iterations",
     "ibfs_last_error",
 ]
 
@@ -86,6 +87,7 @@ def lib():
         L.ibfs_apply_op.argtypes = [vp, ctypes.c_int, _DP, _DP]
         L.ibfs_last_timing.argtypes = [vp, _DP]
         L.ibfs_kernels_per_step.argtypes = [vp]
+        L.ibfs_last_cg_iterations.argtypes = [vp]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
         L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
@@ -215,6 +217,9 @@ class Solver:
         v = ctypes.c_double()
         lib().ibfs_last_timing(self.h, ctypes.byref(v))
         return v.value
+
+    def last_cg_iterations(self):
+        return lib().ibfs_last_cg_iterations(self.h)
 
     def kernels_per_step(self):
         return lib().ibfs_kernels_per_step(self.h)

@@ -139,6 +139,10 @@ int ibfs_last_timing(const ibfs_handle* h, double* ms);
  * counterpart; reports the launch structure of the advance). */
 int ibfs_kernels_per_step(const ibfs_handle* h);
 
+/* CG iterations of the last advance (largest over the handle's cases), as
+ * cjgr reports them (operators.f90:439-440); 0 for Cholesky handles. */
+int ibfs_last_cg_iterations(const ibfs_handle* h);
+
 /* Advances one step without the graph, with CUDA events around every launch
  * on the handle's stream, and returns per launch class the summed device
  * milliseconds, the launch count and the algorithmic flops (arrays of 5):
