@@ -15,9 +15,7 @@
 #include <vector>
 
 #include "../../include/ibfs_capi.h"
-#include "ibfs_common.cuh"
-#include "ibfs_kernels.cuh"
-#include "ibfs_precision.cuh"
+#include "ibfs_handle.cuh"
 
 namespace ibfs {
 
@@ -58,64 +56,11 @@ static double deltafnc(double r, double r0, double dr) {
   return 0.0;
 }
 
-struct HostCase {
-  ibfs_params_c p;
-  ibfs_options_c o;
-  int m, n, L, ns, nq, nb, nf, nring, nbody, bmin;
-  double delta, norm;
-  std::vector<double> xb, yb;
-  std::vector<int> bdyno;
-  std::vector<int> face_ptr, face_f, force_ptr, force_face;
-  std::vector<double> face_w, force_w, wsum;
-  bool have_chol = false;
-  int out_off = 0;
-  int itime = 0;
-  DevCase dc{};
-};
-
 }  // namespace ibfs
 
-using namespace ibfs;
+#include "ibfs_handle.cuh"
 
-struct ibfs_handle {
-  std::vector<HostCase> cases;
-  std::vector<void*> allocs;
-  DevCase* d_cases = nullptr;
-  std::map<int, double*> sine;
-  std::map<int, double*> costab;
-  cudaStream_t st = nullptr;
-  Prog prog;                       // whole step (Cholesky handles) or the part before CG
-  Prog prog_iter, prog_iter50, prog_post;  // CG handles: one iteration, one with residual refresh, after CG
-  cudaGraphExec_t gexec = nullptr, gx_iter = nullptr, gx_iter50 = nullptr, gx_post = nullptr;
-  bool graph_ok = false;
-  int graph_kernels = 0;  // kernel nodes in the captured step graph(s), one CG iteration counted
-  bool cg = false;        // cases solve the force system by CG (stationary = .FALSE.)
-  int* d_cgit = nullptr;  // [ncases][2] iterations, active
-  // a_times shadows of the CG cases: input fb (x) or cg_d (d), private scratch
-  std::vector<DevCase> shx, shd;
-  std::vector<int> cg_ids;
-  DevCase *d_shx = nullptr, *d_shd = nullptr;
-  double* sh_omega = nullptr;
-  size_t sh_omega_bytes = 0;
-  int max_patch = 0, max_nb = 0;
-  std::vector<int> h_cgit;
-  int last_cg_iters = 0;
-  int* d_status = nullptr;
-  int* d_itime = nullptr;
-  double* d_out = nullptr;
-  double* d_hist = nullptr;
-  int hist_steps = 0;
-  int out_stride = 0;
-  double* d_partial = nullptr;
-  std::string err;
-  float last_ms = 0.f;
-  int tile_cfg = -1;
-  int precision = 0;
-  PrecisionPlan* prec = nullptr;
-  int max_ns = 0, max_nq = 0, max_nf = 0, max_ring = 0, max_L = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  double* h_stage = nullptr;  // pinned staging for outputs / body velocities
-};
+using namespace ibfs;
 
 namespace ibfs {
 
@@ -883,9 +828,12 @@ static int finish_create(ibfs_handle* h) {
   return IBFS_OK;
 }
 
+static void free_adj(ibfs_handle* h);
+
 static void free_handle(ibfs_handle* h) {
   if (!h) return;
   if (h->st) cudaStreamSynchronize(h->st);
+  free_adj(h);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->gx_iter) cudaGraphExecDestroy(h->gx_iter);
   if (h->gx_iter50) cudaGraphExecDestroy(h->gx_iter50);
@@ -901,6 +849,19 @@ static void free_handle(ibfs_handle* h) {
 
 static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out);
 
+}  // namespace ibfs
+
+#include "ibfs_adjoint_host.cuh"
+
+namespace ibfs {
+static void free_adj(ibfs_handle* h) {
+  if (!h->adj) return;
+  if (h->adj->g_bw) cudaGraphExecDestroy(h->adj->g_bw);
+  if (h->adj->g_bwf) cudaGraphExecDestroy(h->adj->g_bwf);
+  if (h->adj->h_a) cudaFreeHost(h->adj->h_a);
+  delete h->adj;
+  h->adj = nullptr;
+}
 }  // namespace ibfs
 
 // ===========================================================================
@@ -1092,6 +1053,14 @@ int ibfs_output_stride(const ibfs_handle* h) { return h ? h->out_stride : 0; }
 int ibfs_kernels_per_step(const ibfs_handle* h) { return h ? h->graph_kernels : -1; }
 
 int ibfs_last_cg_iterations(const ibfs_handle* h) { return h ? h->last_cg_iters : -1; }
+
+int ibfs_adjoint_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* body_vel, const double* wx,
+                     const double* wy, double* J, double* grad_vel, double* ms_forward, double* ms_total) {
+  if (!h) return IBFS_ERR_ARG;
+  int rc = adj_run(h, nsteps, checkpoint_every, body_vel, wx, wy, J, grad_vel, ms_forward, ms_total);
+  if (rc) h->err = ibfs_last_error(nullptr);
+  return rc;
+}
 
 int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops) {
   if (!h || !ms || !launches || !flops) return IBFS_ERR_ARG;

@@ -28,6 +28,8 @@ enum GemmEpi {
   EPI_AINV = 2,      // C = lam1i(:,:,1) .* acc / normalize  (ainv, myfft.f90:121)
   EPI_CN = 3,        // C = lam1i_k .* (acc + lam1_k .* acc2)  (operators.f90:126-130)
   EPI_SUBTRACT = 4,  // C = C - acc                          (operators.f90:174)
+  EPI_ADD = 5,       // C = C + acc                          (adjoint accumulation)
+  EPI_ADJ_CN = 6,    // C = lam1i_k .* acc, C2 = lam1i_k .* lam1_k .* acc (adjoint of the CN update)
 };
 
 struct GemmDesc {
@@ -35,6 +37,7 @@ struct GemmDesc {
   const double* B;
   const double* B2;  // second right operand (EPI_CN)
   double* C;
+  double* C2;  // second output (EPI_ADJ_CN)
   int M, N, K, lda, ldb, ldc;
   int pro, epi;
   int m, n, k;             // grid of the node field and its level

@@ -1,0 +1,378 @@
+// k_adjoint.cu -- kernels of the discrete adjoint of one IBFS advance.
+//
+// The forward step (operators.f90:62-188, stationary body, Cholesky solve) is
+// linear in every operator except the bilinear convective term; its adjoint
+// runs the transposed operators in reverse order:
+//   curl^T   = (rot on the nodes, ring terms)     (curl, operators.f90:243-288)
+//   rot^T    = curl with a zero ring              (rot,  operators.f90:291-304)
+//   get_bc^T : ring -> box-perimeter nodes        (get_bc, operators.f90:336-367)
+//   apply_bc^T: edge nodes -> ring                (apply_bc, operators.f90:370-390)
+//   coarsify^T: coarse centre -> fine nodes       (coarsify, operators.f90:307-333)
+//   reg^T = regT, regT^T = reg                    (operators.f90:513-546)
+//   nonlinear: transposed linearisation about the stored forward state
+// The DST-based inverses (ctci, ainv, the CN update) are symmetric and reuse
+// the forward sine-transform GEMMs; the Cholesky solve is symmetric too.
+// All kernels are gathers (no atomics), so the adjoint is deterministic.
+#include "ibfs_adjoint.cuh"
+
+namespace ibfs {
+
+__device__ __forceinline__ int ring_off(int m, int n, int side) {
+  return side == SIDE_LEFT ? 0 : side == SIDE_RIGHT ? n + 1 : side == SIDE_BOTTOM ? 2 * (n + 1) : 2 * (n + 1) + m + 1;
+}
+
+// (s_hat, sbc_hat) = curl^T(q_hat) on level k; zero when k > nlev.
+__global__ void k_adj_curlT(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int nlev,
+                            int use_q1) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int k = blockIdx.y + 1;
+  int m = C.m, n = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const double* Q = use_q1 ? A.aQ1 : A.aQ + (size_t)(k - 1) * C.nq;
+  double* S = A.aS + (size_t)(k - 1) * C.ns;
+  double* R = A.aSbc + (size_t)(k - 1) * C.nring;
+  auto qu = [&](int i, int j) { return Q[uoff(i, j, m)]; };
+  auto qv = [&](int i, int j) { return Q[voff(i, j, m, n)]; };
+  if (t < C.ns) {
+    if (k > nlev) { S[t] = 0.0; return; }
+    int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
+    S[t] = qv(i, j) - qv(i - 1, j) - qu(i, j) + qu(i, j - 1);
+  } else if (t < C.ns + C.nring) {
+    int r = t - C.ns;
+    if (k > nlev) { R[r] = 0.0; return; }
+    double v = 0.0;
+    if (r < n + 1) {  // left, J = r+1
+      int J = r + 1;
+      if (J >= 2) v += qu(1, J - 1);
+      if (J <= n) v -= qu(1, J);
+      if (J >= 2 && J <= n) v += qv(1, J);
+    } else if (r < 2 * (n + 1)) {  // right
+      int J = r - (n + 1) + 1;
+      if (J >= 2) v += qu(m + 1, J - 1);
+      if (J <= n) v -= qu(m + 1, J);
+      if (J >= 2 && J <= n) v -= qv(m, J);
+    } else if (r < 2 * (n + 1) + m + 1) {  // bottom, I
+      int I = r - 2 * (n + 1) + 1;
+      if (I >= 2 && I <= m) v -= qu(I, 1);
+      if (I <= m) v += qv(I, 1);
+      if (I >= 2) v -= qv(I - 1, 1);
+    } else {  // top
+      int I = r - 2 * (n + 1) - (m + 1) + 1;
+      if (I >= 2 && I <= m) v += qu(I, n);
+      if (I <= m) v += qv(I, n + 1);
+      if (I >= 2) v -= qv(I - 1, n + 1);
+    }
+    R[r] = v;
+  }
+}
+
+// apply_bc^T (fac) of a node field into a ring: entry side+I collects the edge
+// node apply_bc adds it to (operators.f90:382-389).
+__device__ __forceinline__ double applybcT_at(const double* __restrict__ x, int m, int n, int r) {
+  auto X = [&](int a, int b) { return x[ridx(a, b, m)]; };
+  if (r < n + 1) { int J = r + 1; return (J >= 2 && J <= n) ? X(1, J - 1) : 0.0; }
+  if (r < 2 * (n + 1)) { int J = r - (n + 1) + 1; return (J >= 2 && J <= n) ? X(m - 1, J - 1) : 0.0; }
+  if (r < 2 * (n + 1) + m + 1) { int I = r - 2 * (n + 1) + 1; return (I >= 2 && I <= m) ? X(I - 1, 1) : 0.0; }
+  int I = r - 2 * (n + 1) - (m + 1) + 1;
+  return (I >= 2 && I <= m) ? X(I - 1, n - 1) : 0.0;
+}
+
+// get_bc^T: the value gathered by coarse node r(a,b) (1-based) from a ring,
+// each ring entry having taken 1 x or 0.5 x of that node (operators.f90:348-366).
+__device__ __forceinline__ double getbcT_at(const double* __restrict__ ring, int m, int n, int a, int b) {
+  double v = 0.0;
+  int bot = 2 * (n + 1), top = bot + m + 1, right = n + 1;
+  if (b == n / 4 || b == 3 * n / 4) {
+    int off = b == n / 4 ? bot : top;
+    int u = a - m / 4;
+    if (u >= 0 && u <= m / 2) {
+      int te = 2 * u;  // even entry t = te
+      v += ring[off + te];
+      if (te - 1 >= 1) v += 0.5 * ring[off + te - 1];
+      if (te + 1 <= m - 1) v += 0.5 * ring[off + te + 1];
+    }
+  }
+  if (a == m / 4 || a == 3 * m / 4) {
+    int off = a == m / 4 ? 0 : right;
+    int u = b - n / 4;
+    if (u >= 0 && u <= n / 2) {
+      int te = 2 * u;
+      v += ring[off + te];
+      if (te - 1 >= 1) v += 0.5 * ring[off + te - 1];
+      if (te + 1 <= n - 1) v += 0.5 * ring[off + te + 1];
+    }
+  }
+  return v;
+}
+
+// aW_k += v ; sbc_hat_k += apply_bc^T(v) (vort2flux adjoint, one level).
+__global__ void k_adj_v2f_level(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const double* v = A.aZ1;
+  if (t < C.ns) {
+    A.aW[(size_t)(k - 1) * C.ns + t] += v[t];
+  } else if (t < C.ns + C.nring) {
+    int r = t - C.ns;
+    A.aSbc[(size_t)(k - 1) * C.nring + r] += applybcT_at(v, C.m, C.n, r);
+  }
+}
+
+// dst(a, b) += fac * get_bc^T(ring) on the box perimeter of a node field.
+__global__ void k_adj_getbcT(const DevCase* __restrict__ cases, const double* __restrict__ ring, double* dst,
+                             double fac) {
+  const DevCase& C = cases[0];
+  int m = C.m, n = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  // perimeter nodes of the box [m/4,3m/4] x [n/4,3n/4]: bottom/top rows, then left/right columns
+  int wa = m / 2 + 1, hb = n / 2 + 1;
+  int a, b;
+  if (t < 2 * wa) { a = m / 4 + t % wa; b = t < wa ? n / 4 : 3 * n / 4; }
+  else if (t < 2 * wa + 2 * (hb - 2)) {
+    int u = t - 2 * wa;
+    a = u < hb - 2 ? m / 4 : 3 * m / 4;
+    b = n / 4 + 1 + u % (hb - 2);
+  } else return;
+  dst[ridx(a, b, m)] += fac * getbcT_at(ring, m, n, a, b);
+}
+
+// coarsify^T (operators.f90:320-332): fine level k-1 gathers the coarse
+// centre of level k with the full-weighting weights; then the centre of
+// level k is cleared (it was overwritten in the forward pass).
+__global__ void k_adj_coarsifyT(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int m = C.m, n = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C.ns) return;
+  int ii = t % (m - 1) + 2, jj = t / (m - 1) + 2;
+  const double* Wc = A.aW + (size_t)(k - 1) * C.ns;
+  double s = 0.0;
+  // coarse i with |ii - (2i - m/2 - 1)| <= 1, i in [m/4+2, 3m/4]
+  for (int di = -1; di <= 1; di++) {
+    int x2 = ii + m / 2 + 1 + di;  // = 2i
+    if (x2 & 1) continue;
+    int i = x2 / 2;
+    if (i < m / 4 + 2 || i > 3 * m / 4) continue;
+    double wi = di == 0 ? 1.0 : 0.5;
+    for (int dj = -1; dj <= 1; dj++) {
+      int y2 = jj + n / 2 + 1 + dj;
+      if (y2 & 1) continue;
+      int j = y2 / 2;
+      if (j < n / 4 + 2 || j > 3 * n / 4) continue;
+      double wj = dj == 0 ? 1.0 : 0.5;
+      s += wi * wj * Wc[nidx(i, j, m)];
+    }
+  }
+  A.aW[(size_t)(k - 2) * C.ns + t] += s;
+}
+
+__global__ void k_adj_zero_centre(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int m = C.m, n = C.n;
+  int ci = 3 * m / 4 - (m / 4 + 2) + 1, cj = 3 * n / 4 - (n / 4 + 2) + 1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ci * cj) return;
+  int i = t % ci + m / 4 + 2, j = t / ci + n / 4 + 2;
+  A.aW[(size_t)(k - 1) * C.ns + nidx(i, j, m)] = 0.0;
+}
+
+// F_hat' = objective term + (-regT(curl0(aZ1))) (projection adjoint,
+// operators.f90:174) ; objective: J += wx_b fx_b + wy_b fy_b with
+// f = 2 delta / dt * sum wsum_f fb_f (write_force).
+__global__ void k_adj_force(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= C.nf) return;
+  int m = C.m, n = C.n;
+  int p = f < C.nb ? f : f - C.nb;
+  int b = C.bdyno[p] - C.bmin;
+  double w = f < C.nb ? A.wx[b] : A.wy[b];
+  double v = w * 2.0 * C.delta / C.dt * C.wsum[f];
+  // regT of curl(x, 0) (x = aZ1, nodes), gathered over the force's faces
+  const double* x = A.aZ1;
+  auto X = [&](int i, int j) { return (i >= 2 && i <= m && j >= 2 && j <= n) ? x[nidx(i, j, m)] : 0.0; };
+  double s = 0.0;
+  for (int q = C.force_ptr[f]; q < C.force_ptr[f + 1]; q++) {
+    int face = C.force_face[q];
+    double cv;
+    int nu = (m + 1) * n;
+    if (face < nu) {
+      int i = face % (m + 1) + 1, j = face / (m + 1) + 1;
+      cv = (i == 1 || i == m + 1) ? 0.0 : X(i, j + 1) - X(i, j);
+    } else {
+      int fv = face - nu, i = fv % m + 1, j = fv / m + 1;
+      cv = (j == 1 || j == n + 1) ? 0.0 : X(i, j) - X(i + 1, j);
+    }
+    s += C.force_w[q] * cv;
+  }
+  A.aF[f] = v - s;
+}
+
+// y = Linv b (lower) / x = LinvT y (upper) on adjoint vectors; warp per row.
+__global__ void k_adj_tri(const DevCase* __restrict__ cases, const double* __restrict__ in, double* out, int upper) {
+  const DevCase& C = cases[0];
+  int nf = C.nf;
+  int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+  if (row >= nf) return;
+  const double* Mr = (upper ? C.LinvT : C.Linv) + (size_t)row * nf;
+  int k0 = upper ? row : 0, k1 = upper ? nf : row + 1;
+  double s = 0.0;
+  for (int k = k0 + lane; k < k1; k += 32) s = fma(Mr[k], in[k], s);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[row] = s;
+}
+
+// q1_hat = reg(rhsf_hat) on all faces; grad_vel -= delta * rhsf_hat
+// (rhsf = regT(q1) - (delta*vel - regT(q0)), operators.f90:155-164).
+__global__ void k_adj_rhsf(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < C.nq) {
+    int p0 = C.face_ptr[t], p1 = C.face_ptr[t + 1];
+    double h = 0.0;
+    for (int p = p0; p < p1; p++) h = h + C.face_w[p] * A.aRf[C.face_f[p]];
+    A.aQ1[t] = h;
+  }
+  if (t < C.nf) A.aGrad[t] -= C.delta * A.aRf[t];
+}
+
+// Level-k CN adjoint, node part: r_hat = con1 A_hat + P_hat' ; P_hat = con2 A_hat
+// (first step: rhs_old was set to rhs, so r_hat += con2 A_hat, P_hat = 0);
+// ring part: lastbc_hat_k += vfac apply_bc^T(A_hat), ob_hat = vfac apply_bc^T(A_hat).
+__global__ void k_adj_level(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k, int first) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double del22 = C.delta * C.delta * (double)(1 << (2 * (k - 1)));
+  double con1 = 1.5 * C.dt / del22 / C.norm, con2 = -0.5 * C.dt / del22 / C.norm;
+  double vf = 0.5 * C.dt / C.re / del22 / C.norm;
+  if (t < C.ns) {
+    double ah = A.aA[t];
+    double* P = A.aP + (size_t)(k - 1) * C.ns;
+    double r = con1 * ah + P[t];
+    if (first) { r += con2 * ah; P[t] = 0.0; }
+    else P[t] = con2 * ah;
+    A.aR[t] = r;
+  } else if (t < C.ns + C.nring) {
+    int r = t - C.ns;
+    double v = vf * applybcT_at(A.aA, C.m, C.n, r);
+    A.aLb[(size_t)(k - 1) * C.nring + r] += v;
+    A.aObc[r] = v;
+  }
+}
+
+// Transposed linearisation of nonlinear(omega, q, q0, bc) followed by rot,
+// about the stored forward state (operators.f90:465-510, 291-304). With
+// H = rot^T r_hat = curl(r_hat, 0):
+//   node  omega_hat(i,j) += .5 va(i,j)(Hu(i,j-1)+Hu(i,j)) - .5 ua(i,j)(Hv(i-1,j)+Hv(i,j))
+//   ring  lastbc_hat     += the same products at the edge entries
+//   face  q_hat           = .5 * (adjoints of the face averages uavg / vavg)
+__global__ void k_adj_nonlinear(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int m = C.m, n = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const double* W = A.fwW + (size_t)(k - 1) * C.ns;
+  const double* Q = A.fwQ + (size_t)(k - 1) * C.nq;
+  const double* Q0 = C.q0 + (size_t)(k - 1) * C.nq;
+  const double* Wc = k < C.L ? A.fwW + (size_t)k * C.ns : nullptr;  // level k+1, for lastbc
+  const double* rh = A.aR;
+  auto bcv = [&](int side, int I) { return Wc ? getbc_raw(Wc, m, n, side, I) * 0.25 : 0.0; };
+  auto R = [&](int i, int j) { return rh[nidx(i, j, m)]; };
+  // H = curl(r_hat, 0): u faces (i=2..m, j=1..n), v faces (i=1..m, j=2..n)
+  auto Hu = [&](int i, int j) -> double {
+    if (i < 2 || i > m || j < 1 || j > n) return 0.0;
+    if (j == 1) return R(i, 2);
+    if (j == n) return -R(i, n);
+    return R(i, j + 1) - R(i, j);
+  };
+  auto Hv = [&](int i, int j) -> double {
+    if (i < 1 || i > m || j < 2 || j > n) return 0.0;
+    if (i == 1) return -R(2, j);
+    if (i == m) return R(m, j);
+    return R(i, j) - R(i + 1, j);
+  };
+  auto qt = [&](int face) { return Q[face] + Q0[face]; };
+  auto va = [&](int i, int j) { return 0.5 * (qt(voff(i, j, m, n)) + qt(voff(i - 1, j, m, n))); };  // i=2..m
+  auto ua = [&](int i, int j) { return 0.5 * (qt(uoff(i, j, m)) + qt(uoff(i, j - 1, m))); };      // j=2..n
+  auto Wj = [&](int i, int j) -> double {  // omega extended along j (column i)
+    if (j == 1) return bcv(SIDE_BOTTOM, i);
+    if (j == n + 1) return bcv(SIDE_TOP, i);
+    return W[nidx(i, j, m)];
+  };
+  auto Wi = [&](int i, int j) -> double {
+    if (i == 1) return bcv(SIDE_LEFT, j);
+    if (i == m + 1) return bcv(SIDE_RIGHT, j);
+    return W[nidx(i, j, m)];
+  };
+  // adjoints of the averages
+  auto vah = [&](int i, int j) { return 0.5 * Wj(i, j) * (Hu(i, j - 1) + Hu(i, j)); };   // i=2..m, j=1..n+1
+  auto uah = [&](int i, int j) { return -0.5 * Wi(i, j) * (Hv(i - 1, j) + Hv(i, j)); };  // i=1..m+1, j=2..n
+  if (t < C.ns) {
+    int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
+    double v = 0.5 * va(i, j) * (Hu(i, j - 1) + Hu(i, j)) - 0.5 * ua(i, j) * (Hv(i - 1, j) + Hv(i, j));
+    A.aW2[(size_t)(k - 1) * C.ns + t] += v;
+  } else if (t < C.ns + C.nq) {
+    int f = t - C.ns, nu = (m + 1) * n;
+    double v = 0.0;
+    if (f < nu) {  // u(i,j): uavg(i,j) [2<=j<=n] and uavg(i,j+1) [j+1<=n]
+      int i = f % (m + 1) + 1, j = f / (m + 1) + 1;
+      if (j >= 2) v += 0.5 * uah(i, j);
+      if (j + 1 <= n) v += 0.5 * uah(i, j + 1);
+    } else {  // v(i,j): vavg(i,j) [2<=i<=m] and vavg(i+1,j) [i+1<=m]
+      int fv = f - nu, i = fv % m + 1, j = fv / m + 1;
+      if (i >= 2) v += 0.5 * vah(i, j);
+      if (i + 1 <= m) v += 0.5 * vah(i + 1, j);
+    }
+    A.aQ[(size_t)(k - 1) * C.nq + f] = v;
+  } else if (t < C.ns + C.nq + C.nring) {
+    int r = t - C.ns - C.nq;
+    double v = 0.0;
+    if (r < n + 1) { int J = r + 1; if (J >= 2 && J <= n) v = -0.5 * ua(1, J) * Hv(1, J); }
+    else if (r < 2 * (n + 1)) { int J = r - (n + 1) + 1; if (J >= 2 && J <= n) v = -0.5 * ua(m + 1, J) * Hv(m, J); }
+    else if (r < 2 * (n + 1) + m + 1) { int I = r - 2 * (n + 1) + 1; if (I >= 2 && I <= m) v = 0.5 * va(I, 1) * Hu(I, 1); }
+    else { int I = r - 2 * (n + 1) - (m + 1) + 1; if (I >= 2 && I <= m) v = 0.5 * va(I, n + 1) * Hu(I, n); }
+    A.aLb[(size_t)(k - 1) * C.nring + r] += v;
+  }
+}
+
+// -------------------------------------------------------------------------
+void adj_curlT(const DevCase* c, const AdjCase* a, const DevCase& h, int nlev, int use_q1, cudaStream_t st) {
+  k_adj_curlT<<<dim3((h.ns + h.nring + 255) / 256, h.L), 256, 0, st>>>(c, a, nlev, use_q1);
+}
+void adj_v2f_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st) {
+  k_adj_v2f_level<<<(h.ns + h.nring + 255) / 256, 256, 0, st>>>(c, a, k);
+}
+void adj_getbcT(const DevCase* c, const double* ring, double* dst, const DevCase& h, double fac, cudaStream_t st) {
+  int np = 2 * (h.m / 2 + 1) + 2 * (h.n / 2 - 1);
+  k_adj_getbcT<<<(np + 255) / 256, 256, 0, st>>>(c, ring, dst, fac);
+}
+void adj_coarsifyT(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st) {
+  k_adj_coarsifyT<<<(h.ns + 255) / 256, 256, 0, st>>>(c, a, k);
+  k_adj_zero_centre<<<(h.ns / 4 + 255) / 256 + 1, 256, 0, st>>>(c, a, k);
+}
+void adj_force(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st) {
+  k_adj_force<<<(h.nf + 127) / 128, 128, 0, st>>>(c, a);
+}
+void adj_solve(const DevCase* c, const double* in, double* tmp, double* out, const DevCase& h, cudaStream_t st) {
+  k_adj_tri<<<(h.nf + 7) / 8, 256, 0, st>>>(c, in, tmp, 0);
+  k_adj_tri<<<(h.nf + 7) / 8, 256, 0, st>>>(c, tmp, out, 1);
+}
+void adj_rhsf(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st) {
+  k_adj_rhsf<<<(h.nq + 255) / 256, 256, 0, st>>>(c, a);
+}
+void adj_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, int first, cudaStream_t st) {
+  k_adj_level<<<(h.ns + h.nring + 255) / 256, 256, 0, st>>>(c, a, k, first);
+}
+void adj_nonlinear(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st) {
+  k_adj_nonlinear<<<(h.ns + h.nq + h.nring + 255) / 256, 256, 0, st>>>(c, a, k);
+}
+
+}  // namespace ibfs

@@ -144,6 +144,8 @@ __global__ void __launch_bounds__(256) k_gemm_f64(const GemmDesc* __restrict__ d
         Cp[o] = x;
       } else if (epi == EPI_SUBTRACT) {
         Cp[o] = Cp[o] - x;
+      } else if (epi == EPI_ADD) {
+        Cp[o] = Cp[o] + x;
       } else {
         double lam = lam_ij(d.cosx[r], d.cosy[c]);
         if (epi == EPI_LAMINV) {
@@ -151,6 +153,12 @@ __global__ void __launch_bounds__(256) k_gemm_f64(const GemmDesc* __restrict__ d
         } else if (epi == EPI_AINV) {
           double l1i = 1.0 / (1.0 + 0.5 * d.dt * lam / d.del22 / d.re);
           Cp[o] = l1i * x / d.norm;
+        } else if (epi == EPI_ADJ_CN) {
+          double nu = 0.5 * d.dt * lam / d.del22 / d.re;
+          double l1 = (1.0 - nu) / d.norm;
+          double l1i = 1.0 / (1.0 + nu);
+          Cp[o] = l1i * x;
+          d.C2[o] = l1i * l1 * x;
         } else {  // EPI_CN
           double nu = 0.5 * d.dt * lam / d.del22 / d.re;
           double l1 = (1.0 - nu) / d.norm;

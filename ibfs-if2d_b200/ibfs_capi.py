@@ -24,7 +24,7 @@ EXPORTS = [
     "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
     "ibfs_advance", "ibfs_advance_n", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
-    "ibfs_last_cg_iterations",
+    "ibfs_last_cg_iterations", "ibfs_adjoint_run",
     "ibfs_last_error",
 ]
 
@@ -88,6 +88,7 @@ def lib():
         L.ibfs_last_timing.argtypes = [vp, _DP]
         L.ibfs_kernels_per_step.argtypes = [vp]
         L.ibfs_last_cg_iterations.argtypes = [vp]
+        L.ibfs_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
         L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
@@ -217,6 +218,19 @@ class Solver:
         v = ctypes.c_double()
         lib().ibfs_last_timing(self.h, ctypes.byref(v))
         return v.value
+
+    def adjoint_run(self, nsteps, checkpoint_every, body_vel, wx, wy):
+        """J and dJ/d body_vel over nsteps advances (see ibfs_adjoint_run)."""
+        nf = self.sizes[0]["nf"]
+        bv = None if body_vel is None else np.ascontiguousarray(body_vel, dtype=np.float64)
+        wx = np.ascontiguousarray(wx, dtype=np.float64)
+        wy = np.ascontiguousarray(wy, dtype=np.float64)
+        J, ms_f, ms_t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        grad = np.zeros(nf)
+        self._check(lib().ibfs_adjoint_run(self.h, nsteps, checkpoint_every, _p(bv), _p(wx), _p(wy),
+                                           ctypes.byref(J), _p(grad), ctypes.byref(ms_f), ctypes.byref(ms_t)))
+        self.itime.value += nsteps
+        return J.value, grad, ms_f.value, ms_t.value
 
     def last_cg_iterations(self):
         return lib().ibfs_last_cg_iterations(self.h)

@@ -139,6 +139,22 @@ int ibfs_last_timing(const ibfs_handle* h, double* ms);
  * counterpart; reports the launch structure of the advance). */
 int ibfs_kernels_per_step(const ibfs_handle* h);
 
+/* Discrete adjoint of nsteps advances (no reference counterpart; the
+ * reference has no derivatives). For a single-case handle, stationary body,
+ * FP64 form: from the current state, with the body velocities body_vel (Nf,
+ * flow units as in ibfs_advance, NULL = 0) held constant, it runs nsteps
+ * advances and returns J = sum_s sum_b (wx[s*nbody+b] fx_b^s + wy[s*nbody+b]
+ * fy_b^s) over the write_force outputs, and grad_vel = dJ/d body_vel (Nf).
+ * Checkpoints of the state every checkpoint_every steps; each segment is
+ * recomputed during the backward pass. The transposed operators: curl^T
+ * (rot and ring terms), rot^T (curl with zero ring), get_bc^T, apply_bc^T,
+ * coarsify^T, reg <-> regT, the linearised nonlinear term transposed; the DST
+ * inverses and the Cholesky solve are self-adjoint. On return the state is
+ * the state after the nsteps advances. ms_forward / ms_total (may be NULL):
+ * device time of the forward pass and of the whole run. */
+int ibfs_adjoint_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* body_vel, const double* wx,
+                     const double* wy, double* J, double* grad_vel, double* ms_forward, double* ms_total);
+
 /* CG iterations of the last advance (largest over the handle's cases), as
  * cjgr reports them (operators.f90:439-440); 0 for Cholesky handles. */
 int ibfs_last_cg_iterations(const ibfs_handle* h);
