@@ -170,6 +170,7 @@ struct __align__(64) TcDesc {
   CUtensorMap mapB;
   int M, N, Kp;   // logical output extents; K padded to a multiple of 64
   int tiles_m, tiles_n, bn;
+  int nprod;      // slice products: 6 (three slices per operand) or 3 (two slices: A0B0 + A0B1 + A1B0)
   int epi, fkind;
   int ldcs, ldc;
   long long sC;
@@ -373,6 +374,192 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const TcDesc* __restrict__ d
 }
 
 // ---------------------------------------------------------------------------
+// Persistent form of the same GEMM (k_gemm_tc_persist): one CTA per SM walks
+// a cost-sorted work list of (desc, tile) items. Warp 0 lane 0 issues the TMA
+// loads, warp 1 lane 0 the tcgen05.mma; the accumulator is double-buffered in
+// TMEM (2 x 128 columns) so warps 2-5 drain tile t (tcgen05.ld + epilogue)
+// while tile t+1 is loaded and multiplied. Per-tile fixed costs (TMEM
+// allocation, pipeline fill, epilogue) are thereby hidden behind the MMAs.
+struct TcWork {
+  int desc, tile;
+};
+
+constexpr int kPStage = 3 * 128 * 64 * 2 + 3 * 128 * 64 * 2;  // 96 KB
+constexpr int kPEpi = 4 * 32 * 33 * 4;                        // per-warp transpose staging
+constexpr int kPSmem = 2 * kPStage + kPEpi + 1024 + 256;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+// Epilogue of one 128x128 tile for one warp (32 rows starting at r0; this
+// lane's row i); trow = TMEM address of the warp's lanes at the accumulator.
+__device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t trow, int i, int r0, int lane,
+                                            float* stg) {
+  const int M = d.M, N = d.N, epi = d.epi, fkind = d.fkind, ldcs = d.ldcs, ldc = d.ldc;
+  const long long sC = d.sC;
+  bf16* const Cs = d.Cs;
+  double* const C64 = d.C64;
+  const float* const lamy = d.lamy;
+  const float nu = d.nu, norm = d.norm;
+  float lx = (epi == TC_SCALE_SPLIT_ROW && i < M) ? __ldg(&d.lamx[i]) : 0.f;
+#pragma unroll 1
+  for (int ch = 0; ch < 4; ch++) {
+    float v[32];
+    tmem_ld32(trow + ch * 32, v);
+    const int jb = n0 + ch * 32;
+    if (epi == TC_SPLIT_COL) {
+#pragma unroll
+      for (int t = 0; t < 32; t++) stg[t * 33 + lane] = v[t];
+      __syncwarp();
+      if (r0 < ldcs) {
+        const int j = jb + lane;
+        bf16 s0[32], s1[32], s2[32];
+#pragma unroll
+        for (int r = 0; r < 32; r++) split3f(stg[lane * 33 + r], s0[r], s1[r], s2[r]);
+        bf16* o = Cs + (size_t)j * ldcs + r0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          store8(o + q * 8, s0 + q * 8);
+          store8(o + sC + q * 8, s1 + q * 8);
+          store8(o + 2 * sC + q * 8, s2 + q * 8);
+        }
+      }
+      __syncwarp();
+    } else if (epi == TC_SCALE_SPLIT_ROW) {
+      if (jb < ldcs) {
+        bf16 s0[32], s1[32], s2[32];
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+          const int j = jb + t;
+          float f = 0.f;
+          if (i < M && j < N) {
+            float lam = lx + __ldg(&lamy[j]);
+            f = fkind == F_LAMINV ? __frcp_rn(lam * norm) : __frcp_rn((1.f + nu * lam) * norm);
+          }
+          split3f(v[t] * f, s0[t], s1[t], s2[t]);
+        }
+        bf16* o = Cs + (size_t)i * ldcs + jb;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          store8(o + q * 8, s0 + q * 8);
+          store8(o + sC + q * 8, s1 + q * 8);
+          store8(o + 2 * sC + q * 8, s2 + q * 8);
+        }
+      }
+    } else if (i < M) {
+#pragma unroll
+      for (int t = 0; t < 32; t++) {
+        const int j = jb + t;
+        if (j < N) {
+          size_t o = (size_t)i + (size_t)j * ldc;
+          C64[o] = epi == TC_F64_ADD ? C64[o] + (double)v[t] : (double)v[t];
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(192, 1) k_gemm_tc_persist(const TcDesc* __restrict__ descs,
+                                                            const TcWork* __restrict__ work, int nwork,
+                                                            int* __restrict__ status) {
+  constexpr int BK = 64, S = 2, AB = 128 * BK * 2, SB = kPStage;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float* stg_all = reinterpret_cast<float*>(smem + S * SB);
+  uint64_t* bars = (uint64_t*)(smem + S * SB + kPEpi);  // full[2] empty[2] accf[2] acce[2]
+  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + kPEpi + 8 * 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]);
+  const uint32_t accf0 = smem_u32(&bars[4]), acce0 = smem_u32(&bars[6]);
+  if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 256);
+  if (tid == 0) {
+    for (int b = 0; b < 6; b++) mbar_init(smem_u32(&bars[b]), 1);
+    for (int b = 6; b < 8; b++) mbar_init(smem_u32(&bars[b]), 4);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int G = gridDim.x;
+  bool to = false;
+
+  if (tid == 0) {  // TMA producer
+    int g = 0;
+    for (int w = blockIdx.x; w < nwork && !to; w += G) {
+      const TcDesc& d = descs[work[w].desc];
+      const int tile = work[w].tile;
+      const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * 128;
+      const int nk = d.Kp / BK;
+      const int ns = d.nprod == 3 ? 2 : 3;  // slices per operand
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g & 1;
+        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g >> 1) + 1) & 1)) { to = true; break; }
+        const uint32_t fb = full0 + 8 * s;
+        mbar_expect_tx(fb, 2 * ns * AB);
+        const uint32_t st = sbase + s * SB;
+        for (int t = 0; t < ns; t++) tma_load_3d(st + t * AB, &d.mapA, kb * BK, m0, t, fb);
+        for (int t = 0; t < ns; t++) tma_load_3d(st + 3 * AB + t * AB, &d.mapB, kb * BK, n0, t, fb);
+      }
+    }
+  } else if (tid == 32) {  // MMA issuer
+    const int pa[6] = {0, 0, 1, 0, 1, 2};
+    const int pb[6] = {0, 1, 0, 2, 1, 0};
+    int g = 0, t = 0;
+    for (int w = blockIdx.x; w < nwork && !to; w += G, t++) {
+      const int a = t & 1, u = t >> 1;
+      if (t >= 2 && !mbar_spin(acce0 + 8 * a, (u - 1) & 1)) { to = true; break; }
+      tc_fence_after();
+      const TcDesc& d = descs[work[w].desc];
+      const int nk = d.Kp / BK;
+      const int np = d.nprod == 3 ? 3 : 6;
+      const uint32_t acc = tmem + a * 128;
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g & 1;
+        if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1)) { to = true; break; }
+        tc_fence_after();
+        const uint32_t st = sbase + s * SB;
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+          if (p >= np) break;
+#pragma unroll
+          for (int k16 = 0; k16 < BK / 16; k16++) {
+            uint64_t da = smem_desc_kmajor<BK>(st + pa[p] * AB + k16 * 32);
+            uint64_t db = smem_desc_kmajor<BK>(st + 3 * AB + pb[p] * AB + k16 * 32);
+            umma_bf16<128>(acc, da, db, (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
+          }
+        }
+        umma_commit(empty0 + 8 * s);
+      }
+      if (!to) umma_commit(accf0 + 8 * a);
+    }
+  } else if (warp >= 2) {  // epilogue warps
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    float* stg = stg_all + (warp - 2) * (32 * 33);
+    int t = 0;
+    for (int w = blockIdx.x; w < nwork; w += G, t++) {
+      const int a = t & 1, u = t >> 1;
+      if (!mbar_wait(accf0 + 8 * a, u & 1)) { to = true; break; }
+      tc_fence_after();
+      const TcDesc& d = descs[work[w].desc];
+      const int tile = work[w].tile;
+      const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * 128;
+      const int r0 = m0 + 32 * q;
+      tc_epilogue(d, n0, tmem + a * 128 + ((uint32_t)(32 * q) << 16), r0 + lane, r0, lane, stg);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce0 + 8 * a);
+    }
+  }
+  __syncwarp();
+  if (__syncthreads_or(to) && tid == 0) atomicOr(status, 2);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// ---------------------------------------------------------------------------
 // FP64 source / residual assembly, split into row-major BF16 slices [i][j]
 // through a 32x32 shared-memory transpose.
 enum ResKind { RES_NONE = 0, RES_LAP = 1, RES_AOP = 2 };
@@ -486,6 +673,8 @@ struct PrecisionPlan {
 };
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static bool g_persist = true;  // persistent GEMM (default) or one CTA per tile
+static int g_num_sms = 0;
 
 static inline int rup(int x, int a) { return (x + a - 1) / a * a; }
 
@@ -566,11 +755,17 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
     if (cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()) !=
             cudaSuccess ||
         cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<256>()) !=
-            cudaSuccess) {
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, kPSmem) != cudaSuccess) {
       g_perr = "cannot raise shared memory limit for the tensor-core GEMM";
       return 4;
     }
     attr = true;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    const char* env = getenv("IBFS_TC_PER_TILE");
+    if (env && env[0] == '1') g_persist = false;
   }
   pp->status = cases.empty() ? (int*)alloc(sizeof(int) * 4) : cases[0].status;
   if (!g_encode) {
@@ -636,7 +831,31 @@ static T* upload(PrecisionPlan* pp, const std::vector<T>& v) {
   return p;
 }
 
+// One persistent launch over every tile of every descriptor, work items
+// sorted by K length (longest first) for balance across the SMs.
+static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& ds, cudaStream_t st) {
+  if (ds.empty()) return;
+  std::vector<TcWork> wl;
+  double fl = 0.0;
+  for (int i = 0; i < (int)ds.size(); i++) {
+    for (int t = 0; t < ds[i].tiles_m * ds[i].tiles_n; t++) wl.push_back({i, t});
+    const TcDesc& d = ds[i];
+    fl += 2.0 * d.M * (double)d.N * (double)(d.epi == TC_SPLIT_COL ? d.N : d.M);
+  }
+  std::stable_sort(wl.begin(), wl.end(), [&](const TcWork& x, const TcWork& y) { return ds[x.desc].Kp > ds[y.desc].Kp; });
+  TcDesc* dd = upload(pp, ds);
+  TcWork* dw = upload(pp, wl);
+  int nw = (int)wl.size();
+  int grid = std::min(nw, g_num_sms > 0 ? g_num_sms : 148);
+  int* status = pp->status;
+  P.push_back({[=]() { k_gemm_tc_persist<<<grid, 192, kPSmem, st>>>(dd, dw, nw, status); }, TAG_GEMM_TC, fl});
+}
+
 static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all, cudaStream_t st) {
+  if (g_persist) {
+    add_gemm_persist(pp, P, all, st);
+    return;
+  }
   for (int bn : {128, 256}) {
     std::vector<TcDesc> ds;
     for (auto& d : all) if (d.bn == bn) ds.push_back(d);
@@ -709,6 +928,13 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       TcDesc L2 = L1;  // x = S_m * T'
       L2.epi = pass == 0 ? TC_F64_STORE : TC_F64_ADD;
       L2.C64 = r.out; L2.ldc = M;
+      // the correction solve acts on a residual already ~1e-6 of the data:
+      // two slices per operand (three products, ~1e-5) keep the refined error
+      // at ~1e-11 while halving the work of that pass
+      int np = pass == 0 ? 6 : 3;
+      R.nprod = np;
+      L1.nprod = np;
+      L2.nprod = np;
       g1.push_back(R);
       g2.push_back(L1);
       g3.push_back(R);
