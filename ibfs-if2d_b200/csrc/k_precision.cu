@@ -385,82 +385,114 @@ struct TcWork {
 };
 
 constexpr int kPStage = 3 * 128 * 64 * 2 + 3 * 128 * 64 * 2;  // 96 KB
-constexpr int kPEpi = 4 * 32 * 33 * 4;                        // per-warp transpose staging
+constexpr int kPEpiWarps = 8;                                  // two warps per TMEM lane quarter
+constexpr int kPThreads = 64 + 32 * kPEpiWarps;
+constexpr int kPEpi = kPEpiWarps * 32 * 33 * 4;                // per-warp 32 x 33 FP32 staging
 constexpr int kPSmem = 2 * kPStage + kPEpi + 1024 + 256;
+static_assert(kPSmem <= 232448, "persistent GEMM shared memory above the per-CTA limit");
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
 }
 
-// Epilogue of one 128x128 tile for one warp (32 rows starting at r0; this
-// lane's row i); trow = TMEM address of the warp's lanes at the accumulator.
-__device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t trow, int i, int r0, int lane,
-                                            float* stg) {
+// Epilogue of chunks [c0, c1) (32 columns each) of one 128x128 tile for one
+// warp: 32 rows starting at r0, this lane's row i = r0 + lane; trow = TMEM
+// address of the warp's lanes at the accumulator; stg = the warp's 32 x 33
+// FP32 staging area. Split outputs are restaged so that every warp store
+// writes eight whole 64-byte row segments (lane L: segment L / 4 + 8 k, 16-byte
+// part L % 4); FP64 outputs are column-major, so a warp store of one column
+// is 32 consecutive doubles.
+__device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t trow, int r0, int lane, float* stg,
+                                            int c0, int c1) {
   const int M = d.M, N = d.N, epi = d.epi, fkind = d.fkind, ldcs = d.ldcs, ldc = d.ldc;
   const long long sC = d.sC;
   bf16* const Cs = d.Cs;
   double* const C64 = d.C64;
-  const float* const lamy = d.lamy;
-  const float nu = d.nu, norm = d.norm;
-  float lx = (epi == TC_SCALE_SPLIT_ROW && i < M) ? __ldg(&d.lamx[i]) : 0.f;
+  const int i = r0 + lane;
+  const int seg = lane >> 2, part = lane & 3;
+  float lx = 0.f, nu = 0.f, norm = 1.f;
+  const float* lamy = nullptr;
+  if (epi == TC_SCALE_SPLIT_ROW) {
+    lx = i < M ? __ldg(&d.lamx[i]) : 0.f;
+    nu = d.nu;
+    norm = d.norm;
+    lamy = d.lamy;
+  }
 #pragma unroll 1
-  for (int ch = 0; ch < 4; ch++) {
+  for (int ch = c0; ch < c1; ch++) {
     float v[32];
     tmem_ld32(trow + ch * 32, v);
     const int jb = n0 + ch * 32;
     if (epi == TC_SPLIT_COL) {
+      // output Cs[j][i] (i contiguous): stage column-major, then lane writes
+      // column jb + seg + 8k, rows r0 + 8 part .. + 7
 #pragma unroll
       for (int t = 0; t < 32; t++) stg[t * 33 + lane] = v[t];
       __syncwarp();
       if (r0 < ldcs) {
-        const int j = jb + lane;
-        bf16 s0[32], s1[32], s2[32];
+#pragma unroll 1
+        for (int k = 0; k < 4; k++) {
+          const int c = seg + 8 * k;
+          bf16 s0[8], s1[8], s2[8];
 #pragma unroll
-        for (int r = 0; r < 32; r++) split3f(stg[lane * 33 + r], s0[r], s1[r], s2[r]);
-        bf16* o = Cs + (size_t)j * ldcs + r0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          store8(o + q * 8, s0 + q * 8);
-          store8(o + sC + q * 8, s1 + q * 8);
-          store8(o + 2 * sC + q * 8, s2 + q * 8);
+          for (int e = 0; e < 8; e++) split3f(stg[c * 33 + part * 8 + e], s0[e], s1[e], s2[e]);
+          bf16* o = Cs + (size_t)(jb + c) * ldcs + r0 + part * 8;
+          store8(o, s0);
+          store8(o + sC, s1);
+          store8(o + 2 * sC, s2);
         }
       }
       __syncwarp();
     } else if (epi == TC_SCALE_SPLIT_ROW) {
-      if (jb < ldcs) {
-        bf16 s0[32], s1[32], s2[32];
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-          const int j = jb + t;
-          float f = 0.f;
-          if (i < M && j < N) {
-            float lam = lx + __ldg(&lamy[j]);
-            f = fkind == F_LAMINV ? __frcp_rn(lam * norm) : __frcp_rn((1.f + nu * lam) * norm);
-          }
-          split3f(v[t] * f, s0[t], s1[t], s2[t]);
-        }
-        bf16* o = Cs + (size_t)i * ldcs + jb;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          store8(o + q * 8, s0 + q * 8);
-          store8(o + sC + q * 8, s1 + q * 8);
-          store8(o + 2 * sC + q * 8, s2 + q * 8);
-        }
-      }
-    } else if (i < M) {
+      // output Cs[i][j] (j contiguous): scale, stage row-major, then lane
+      // writes row r0 + seg + 8k, columns jb + 8 part .. + 7
+      const float ly = (jb + lane < N) ? __ldg(&lamy[jb + lane]) : 0.f;
 #pragma unroll
       for (int t = 0; t < 32; t++) {
-        const int j = jb + t;
-        if (j < N) {
-          size_t o = (size_t)i + (size_t)j * ldc;
-          C64[o] = epi == TC_F64_ADD ? C64[o] + (double)v[t] : (double)v[t];
+        const float lam = lx + __shfl_sync(0xffffffffu, ly, t);
+        const float den = fkind == F_LAMINV ? lam * norm : (1.f + nu * lam) * norm;
+        const bool in = i < M && jb + t < N;
+        stg[lane * 33 + t] = in ? __fdividef(v[t], den) : 0.f;
+      }
+      __syncwarp();
+      if (jb < ldcs) {
+#pragma unroll 1
+        for (int k = 0; k < 4; k++) {
+          const int rr = seg + 8 * k;
+          bf16 s0[8], s1[8], s2[8];
+#pragma unroll
+          for (int e = 0; e < 8; e++) split3f(stg[rr * 33 + part * 8 + e], s0[e], s1[e], s2[e]);
+          bf16* o = Cs + (size_t)(r0 + rr) * ldcs + jb + part * 8;
+          store8(o, s0);
+          store8(o + sC, s1);
+          store8(o + 2 * sC, s2);
         }
+      }
+      __syncwarp();
+    } else if (i < M) {
+      if (epi == TC_F64_ADD) {
+        // all loads first: a load after a store to the same array would
+        // otherwise wait for it, one round trip per column
+#pragma unroll
+        for (int h = 0; h < 32; h += 16) {
+          double old[16];
+#pragma unroll
+          for (int t = 0; t < 16; t++)
+            old[t] = (jb + h + t < N) ? C64[(size_t)i + (size_t)(jb + h + t) * ldc] : 0.0;
+#pragma unroll
+          for (int t = 0; t < 16; t++)
+            if (jb + h + t < N) C64[(size_t)i + (size_t)(jb + h + t) * ldc] = old[t] + (double)v[h + t];
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < 32; t++)
+          if (jb + t < N) C64[(size_t)i + (size_t)(jb + t) * ldc] = (double)v[t];
       }
     }
   }
 }
 
-__global__ void __launch_bounds__(192, 1) k_gemm_tc_persist(const TcDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* __restrict__ descs,
                                                             const TcWork* __restrict__ work, int nwork,
                                                             int* __restrict__ status) {
   constexpr int BK = 64, S = 2, AB = 128 * BK * 2, SB = kPStage;
@@ -476,7 +508,7 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tc_persist(const TcDesc* __rest
   if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 256);
   if (tid == 0) {
     for (int b = 0; b < 6; b++) mbar_init(smem_u32(&bars[b]), 1);
-    for (int b = 6; b < 8; b++) mbar_init(smem_u32(&bars[b]), 4);
+    for (int b = 6; b < 8; b++) mbar_init(smem_u32(&bars[b]), kPEpiWarps);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
@@ -504,8 +536,11 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tc_persist(const TcDesc* __rest
       }
     }
   } else if (tid == 32) {  // MMA issuer
-    const int pa[6] = {0, 0, 1, 0, 1, 2};
-    const int pb[6] = {0, 1, 0, 2, 1, 0};
+    constexpr int pa[6] = {0, 0, 1, 0, 1, 2};
+    constexpr int pb[6] = {0, 1, 0, 2, 1, 0};
+    // the stage ring ends below 2^18 bytes, so the 14-bit address field of
+    // the descriptor never carries into the next field
+    const uint64_t d0 = smem_desc_kmajor<BK>(sbase);
     int g = 0, t = 0;
     for (int w = blockIdx.x; w < nwork && !to; w += G, t++) {
       const int a = t & 1, u = t >> 1;
@@ -519,23 +554,25 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tc_persist(const TcDesc* __rest
         const int s = g & 1;
         if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1)) { to = true; break; }
         tc_fence_after();
-        const uint32_t st = sbase + s * SB;
+        // stage base descriptor; operand tiles and K steps are immediate
+        // offsets (16-byte units) on its address field
+        const uint64_t ds = d0 + (uint64_t)((uint32_t)(s * SB) >> 4);
 #pragma unroll
         for (int p = 0; p < 6; p++) {
           if (p >= np) break;
 #pragma unroll
-          for (int k16 = 0; k16 < BK / 16; k16++) {
-            uint64_t da = smem_desc_kmajor<BK>(st + pa[p] * AB + k16 * 32);
-            uint64_t db = smem_desc_kmajor<BK>(st + 3 * AB + pb[p] * AB + k16 * 32);
-            umma_bf16<128>(acc, da, db, (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
-          }
+          for (int k16 = 0; k16 < BK / 16; k16++)
+            umma_bf16<128>(acc, ds + (uint64_t)((pa[p] * AB + k16 * 32) >> 4),
+                           ds + (uint64_t)((3 * AB + pb[p] * AB + k16 * 32) >> 4),
+                           (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
         }
         umma_commit(empty0 + 8 * s);
       }
       if (!to) umma_commit(accf0 + 8 * a);
     }
   } else if (warp >= 2) {  // epilogue warps
-    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int q = warp & 3;              // TMEM lane quarter this warp may access
+    const int c0 = ((warp - 2) >> 2) * 2;  // the warp's two 32-column chunks
     float* stg = stg_all + (warp - 2) * (32 * 33);
     int t = 0;
     for (int w = blockIdx.x; w < nwork; w += G, t++) {
@@ -546,7 +583,7 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tc_persist(const TcDesc* __rest
       const int tile = work[w].tile;
       const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * 128;
       const int r0 = m0 + 32 * q;
-      tc_epilogue(d, n0, tmem + a * 128 + ((uint32_t)(32 * q) << 16), r0 + lane, r0, lane, stg);
+      tc_epilogue(d, n0, tmem + a * 128 + ((uint32_t)(32 * q) << 16), r0, lane, stg, c0, c0 + 2);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce0 + 8 * a);
@@ -848,7 +885,7 @@ static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDes
   int nw = (int)wl.size();
   int grid = std::min(nw, g_num_sms > 0 ? g_num_sms : 148);
   int* status = pp->status;
-  P.push_back({[=]() { k_gemm_tc_persist<<<grid, 192, kPSmem, st>>>(dd, dw, nw, status); }, TAG_GEMM_TC, fl});
+  P.push_back({[=]() { k_gemm_tc_persist<<<grid, kPThreads, kPSmem, st>>>(dd, dw, nw, status); }, TAG_GEMM_TC, fl});
 }
 
 static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all, cudaStream_t st) {
