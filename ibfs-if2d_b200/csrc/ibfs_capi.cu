@@ -199,6 +199,11 @@ struct ProgBuilder {
     add([=]() { launch_gemm_f64(dd, nd, mt, cfg, dual, st); }, TAG_GEMM_F64, fl);
   }
   const LevelItem* items(const std::vector<LevelItem>& v) { return dupload(h, v); }
+  // block map of a grouped element-wise launch from its items' element counts
+  std::pair<const int2*, int> bmap(const std::vector<int>& counts) {
+    std::vector<int2> v = block_map(counts);
+    return {dupload(h, v), (int)v.size()};
+  }
   const int* ints(const std::vector<int>& v) { return dupload(h, v); }
 };
 
@@ -236,11 +241,13 @@ static void build_vort2flux(ProgBuilder& B, const DevCase* dcases, const std::ve
   for (auto& c : cs) { Lmax = std::max(Lmax, c.L); mns = std::max(mns, c.ns); mnq = std::max(mnq, c.nq); }
   for (int k = 2; k <= Lmax; k++) {
     std::vector<LevelItem> it;
-    for (size_t i = 0; i < cs.size(); i++) if (cs[i].L >= k) it.push_back({ids[i], k});
+    std::vector<int> cnt;
+    for (size_t i = 0; i < cs.size(); i++)
+      if (cs[i].L >= k) { it.push_back({ids[i], k}); cnt.push_back(coarsify_count(cs[i].m, cs[i].n)); }
     if (it.empty()) continue;
     const LevelItem* d = B.items(it);
-    int ni = (int)it.size();
-    B.add([=]() { launch_coarsify(dcases, d, ni, mns, st); });
+    auto bm = B.bmap(cnt);
+    B.add([=]() { launch_coarsify(dcases, d, bm.first, bm.second, st); });
   }
   for (int t = 0; t < Lmax; t++) {
     std::vector<GemmDesc> r1, l1, r2, l2;
@@ -262,11 +269,12 @@ static void build_vort2flux(ProgBuilder& B, const DevCase* dcases, const std::ve
     B.gemm(l2, false);
   }
   std::vector<LevelItem> ci;
+  std::vector<int> cnt;
   for (size_t i = 0; i < cs.size(); i++)
-    for (int k = 1; k <= (curl_all ? cs[i].L : 1); k++) ci.push_back({ids[i], k});
+    for (int k = 1; k <= (curl_all ? cs[i].L : 1); k++) { ci.push_back({ids[i], k}); cnt.push_back(cs[i].nq); }
   const LevelItem* d = B.items(ci);
-  int ni = (int)ci.size();
-  B.add([=]() { launch_curl(dcases, d, ni, mnq, st); });
+  auto bm = B.bmap(cnt);
+  B.add([=]() { launch_curl(dcases, d, bm.first, bm.second, st); });
 }
 
 // ainv(x) on level 1 (myfft.f90:112-124): x in c.vort, result stored (or
@@ -299,7 +307,10 @@ static void build_atimes_on(ProgBuilder& B, ibfs_handle* h, const DevCase* dsh, 
   std::vector<int> ids(n);
   for (int i = 0; i < n; i++) { ids[i] = i; mns = std::max(mns, sh[i].ns); mnf = std::max(mnf, sh[i].nf); }
   const int* dids = B.ints(ids);
-  B.add([=]() { launch_regrot(dsh, dids, n, mns, st); }, TAG_CHOL);
+  std::vector<int> cnt(n);
+  for (int i = 0; i < n; i++) cnt[i] = sh[i].ns;
+  auto bm = B.bmap(cnt);
+  B.add([=]() { launch_regrot(dsh, dids, bm.first, bm.second, st); }, TAG_CHOL);
   build_ainv(B, sh, EPI_STORE);
   build_vort2flux(B, dsh, sh, ids, false);
   B.add([=]() { launch_regT_out(dsh, dids, n, mnf, d_out, st); }, TAG_CHOL);
@@ -344,12 +355,14 @@ static void build_step_program(ibfs_handle* h) {
   } else {
     for (int t = 0; t < Lmax; t++) {
       std::vector<LevelItem> it;
+      std::vector<int> cnt;
       std::vector<GemmDesc> r1, l1, r2, l2;
       for (int i = 0; i < nc; i++) {
         const DevCase& c = cs[i];
         int k = c.L - t;
         if (k < 1) continue;
         it.push_back({i, k});
+        cnt.push_back(c.ns);
         double* om = c.omega + (size_t)(k - 1) * c.ns;
         r1.push_back(right_desc(c, c.rhsA, c.wa));
         r1.push_back(right_desc(c, om, c.wb));
@@ -360,8 +373,8 @@ static void build_step_program(ibfs_handle* h) {
         l2.push_back(left_desc(c, c.wa, om, EPI_STORE, k));
       }
       const LevelItem* d = B.items(it);
-      int ni = (int)it.size();
-      B.add([=]() { launch_rhs(dcases, d, ni, mns, 0, st); });
+      auto bm = B.bmap(cnt);
+      B.add([=]() { launch_rhs(dcases, d, bm.first, bm.second, 0, st); });
       B.gemm(r1, false);
       B.gemm(l1, true);
       B.gemm(r2, false);
@@ -405,7 +418,10 @@ static void build_step_program(ibfs_handle* h) {
   }
   ProgBuilder Bp{h, h->cg ? h->prog_post : h->prog};
   // STEP 3 (operators.f90:174)
-  Bp.add([=]() { launch_regrot(dcases, d_ids, nc, mns, st); });
+  std::vector<int> ns_all(nc);
+  for (int i = 0; i < nc; i++) ns_all[i] = cs[i].ns;
+  auto bm_all = Bp.bmap(ns_all);
+  Bp.add([=]() { launch_regrot(dcases, d_ids, bm_all.first, bm_all.second, st); });
   if (h->precision == 1) build_precision_ainv(h->prec, Bp.P, dcases, cs, EPI_SUBTRACT, st);
   else build_ainv(Bp, cs, EPI_SUBTRACT);
   // STEP 4 (operators.f90:177)
@@ -567,7 +583,10 @@ static int precompute(ibfs_handle* h) {
     double** douts = dupload(&tmp, outs);
     cudaStream_t st = h->st;
     B.add([=]() { launch_unit_fb(dsh, dids, dcols, nr, mnf, st); });
-    B.add([=]() { launch_regrot(dsh, dids, nr, mns, st); });
+    std::vector<int> cnt(nr);
+    for (int r = 0; r < nr; r++) cnt[r] = sh[r].ns;
+    auto bm = B.bmap(cnt);
+    B.add([=]() { launch_regrot(dsh, dids, bm.first, bm.second, st); });
     // A is always built in FP64 (the force system stays FP64 in every form)
     build_ainv(B, sh, EPI_STORE);
     build_vort2flux(B, dsh, sh, ids, false);
@@ -1160,7 +1179,8 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
     in_n = c.nf; out_n = c.nf;
     IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
     IBFS_CUDA_CHECK(cudaMemset(s.omega, 0, (size_t)c.L * ns * sizeof(double)));
-    B.add([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
+    auto bm1 = B.bmap({(int)ns});
+    B.add([=]() { launch_regrot(ds, dids, bm1.first, bm1.second, st); });
     if (h->precision == 1) build_precision_ainv(h->prec, P, ds, sv, EPI_STORE, st);
     else build_ainv(B, sv, EPI_STORE);
     if (h->precision == 1) build_precision_vort2flux(h->prec, P, ds, sv, ids, false, st);
@@ -1182,7 +1202,8 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
   } else if (op == 5) {  // rot(reg(f))
     in_n = c.nf; out_n = ns;
     IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
-    B.add([=]() { launch_regrot(ds, dids, 1, (int)ns, st); });
+    auto bm1 = B.bmap({(int)ns});
+    B.add([=]() { launch_regrot(ds, dids, bm1.first, bm1.second, st); });
     dout = s.vort;
   } else {
     rc = fail(IBFS_ERR_ARG, "unknown op");

@@ -52,10 +52,19 @@ int gemm_tiles(int M, int N, int tile_cfg);
 void gemm_f64_init();
 
 void launch_lastbc(const DevCase* cases, const LevelItem* items, int nitems, int max_ring, cudaStream_t st);
-void launch_rhs(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, int first, cudaStream_t st);
-void launch_coarsify(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, cudaStream_t st);
-void launch_curl(const DevCase* cases, const LevelItem* items, int nitems, int max_nq, cudaStream_t st);
-void launch_regrot(const DevCase* cases, const int* cids, int ncases, int max_ns, cudaStream_t st);
+// Grouped element-wise launches: block b of a launch covers elements
+// [map[b].y, map[b].y + kBlockElems) of item map[b].x (block_map(counts)).
+constexpr int kBlockElems = 1024;
+std::vector<int2> block_map(const std::vector<int>& counts);
+// interior nodes coarsify writes on level k > 1 (operators.f90:307-333)
+__host__ __device__ inline int coarsify_count(int m, int n) {
+  return (3 * m / 4 - (m / 4 + 2) + 1) * (3 * n / 4 - (n / 4 + 2) + 1);
+}
+void launch_rhs(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, int first,
+                cudaStream_t st);
+void launch_coarsify(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, cudaStream_t st);
+void launch_curl(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, cudaStream_t st);
+void launch_regrot(const DevCase* cases, const int* cids, const int2* bmap, int nblocks, cudaStream_t st);
 void launch_rhsf(const DevCase* cases, const int* cids, int ncases, int max_nf, cudaStream_t st);
 void launch_regT_out(const DevCase* cases, const int* cids, int ncases, int max_nf, double* const* outs,
                      cudaStream_t st);

@@ -212,6 +212,12 @@ __device__ __forceinline__ void split3f(float x, bf16& s0, bf16& s1, bf16& s2) {
   s2 = __float2bfloat16_rn(r);
 }
 
+__device__ __forceinline__ void store4(bf16* dst, const bf16* v) {
+  uint2 u;
+  u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
+  u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
+  *reinterpret_cast<uint2*>(dst) = u;
+}
 __device__ __forceinline__ void store8(bf16* dst, const bf16* v) {
   uint4 u;
   u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
@@ -628,11 +634,18 @@ __device__ __forceinline__ double lap5(const double* __restrict__ x, int i, int 
   return s;
 }
 
-__global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__ descs) {
-  const PrepDesc& d = descs[blockIdx.z];
+// One 32 x 32 tile of one descriptor per block (block map entry {desc, tile},
+// tiles numbered i-fastest). v is assembled column-major (a warp reads 32
+// consecutive i), staged in shared memory, and written row-major as three BF16
+// slices, four consecutive j per thread (8-byte stores; a warp writes four
+// 64-byte row segments per slice).
+__global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__ descs,
+                                                    const int2* __restrict__ bmap) {
+  const int2 bm = bmap[blockIdx.x];
+  const PrepDesc& d = descs[bm.x];
   const int M = d.m - 1, N = d.n - 1;
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
-  if (i0 >= M || j0 >= N) return;
+  const int ti = (M + 31) / 32;
+  const int i0 = (bm.y % ti) * 32, j0 = (bm.y / ti) * 32;
   __shared__ double t[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   for (int jj = ty; jj < 32; jj += 8) {
@@ -657,16 +670,19 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
     t[jj][tx] = v;
   }
   __syncthreads();
-  for (int ii = ty; ii < 32; ii += 8) {
-    int i = i0 + ii, j = j0 + tx;
-    if (i < M && j < N) {
-      bf16 a, b, c;
-      split3(t[tx][ii], a, b, c);
-      size_t o = (size_t)i * d.ld + j;
-      d.Xs[o] = a;
-      d.Xs[o + d.sX] = b;
-      d.Xs[o + 2 * d.sX] = c;
-    }
+  const int ii = threadIdx.x >> 3, g = threadIdx.x & 7;  // row ii, columns 4g .. 4g+3
+  const int i = i0 + ii, j = j0 + 4 * g;
+  if (i < M && j < N) {
+    bf16 a[4], b[4], c[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) split3(t[4 * g + e][ii], a[e], b[e], c[e]);
+    bf16* o = d.Xs + (size_t)i * d.ld + j;
+    // the row stride and the slice stride are multiples of 64 elements, so
+    // every 4-element group starts 8-byte aligned; columns >= N of the last
+    // group are zero (the padding the GEMM reads as K)
+    store4(o, a);
+    store4(o + d.sX, b);
+    store4(o + 2 * d.sX, c);
   }
 }
 
@@ -859,6 +875,7 @@ struct SolveReq {
   int fkind;          // F_LAMINV (ctci) or F_LAM1I_NORM (A = I + nu C^T C)
   PrepDesc src;       // how to assemble v (Xs and ld filled in here)
   double* out;        // x (column-major FP64)
+  bool presplit;      // v's slices are already in the case's X buffer: pass 0 needs no assembly
 };
 
 template <class T>
@@ -915,18 +932,15 @@ static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all,
 
 static void add_prep(PrecisionPlan* pp, Prog& P, const std::vector<PrepDesc>& ds, cudaStream_t st) {
   if (ds.empty()) return;
-  int gx = 0, gy = 0;
-  for (auto& d : ds) {
-    gx = std::max(gx, (d.m - 1 + 31) / 32);
-    gy = std::max(gy, (d.n - 1 + 31) / 32);
+  std::vector<int2> map;
+  for (int i = 0; i < (int)ds.size(); i++) {
+    int tiles = ((ds[i].m - 1 + 31) / 32) * ((ds[i].n - 1 + 31) / 32);
+    for (int t = 0; t < tiles; t++) map.push_back(make_int2(i, t));
   }
   PrepDesc* dd = upload(pp, ds);
-  int nd = (int)ds.size();
-  P.push_back({[=]() {
-                 dim3 g(gx, gy, nd);
-                 k_prep_split<<<g, 256, 0, st>>>(dd);
-               },
-               TAG_SPLIT, 0.0});
+  const int2* dm = upload(pp, map);
+  const int nb = (int)map.size();
+  P.push_back({[=]() { k_prep_split<<<nb, 256, 0, st>>>(dd, dm); }, TAG_SPLIT, 0.0});
 }
 
 // The eight GEMMs + two assembly passes of a batch of refined solves.
@@ -949,7 +963,7 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       } else {
         pd.x0 = nullptr;
       }
-      prep.push_back(pd);
+      if (!(pass == 0 && r.presplit)) prep.push_back(pd);
       int M = c.m - 1, N = c.n - 1;
       int tm = (M + 127) / 128, tn = (N + b.bn - 1) / b.bn;
       TcDesc R{};  // T = X * S_n
@@ -991,12 +1005,14 @@ void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, co
   for (auto& c : cs) { Lmax = std::max(Lmax, c.L); mns = std::max(mns, c.ns); }
   for (int t = 0; t < Lmax; t++) {
     std::vector<LevelItem> it;
+    std::vector<int> cnt;
     std::vector<SolveReq> rq;
     for (size_t i = 0; i < cs.size(); i++) {
       const DevCase& c = cs[i];
       int k = c.L - t;
       if (k < 1) continue;
       it.push_back({(int)i, k});
+      cnt.push_back(c.ns);
       // b = norm*rhsA + (I - nu_k C^T C) omega_k ; omega_k <- A_k^-1 b
       SolveReq r{};
       r.c = (int)i; r.hc = &cs[i]; r.k = k; r.fkind = F_LAM1I_NORM;
@@ -1008,8 +1024,10 @@ void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, co
       rq.push_back(r);
     }
     LevelItem* d_it = upload(pp, it);
-    int ni = (int)it.size();
-    P.push_back({[=]() { launch_rhs(dcases, d_it, ni, mns, 0, st); }, TAG_STENCIL, 0.0});
+    const std::vector<int2> bmv = block_map(cnt);
+    const int2* bm = upload(pp, bmv);
+    const int nbm = (int)bmv.size();
+    P.push_back({[=]() { launch_rhs(dcases, d_it, bm, nbm, 0, st); }, TAG_STENCIL, 0.0});
     // b must be formed before omega_k is overwritten by x0: keep b in wd
     std::vector<PrepDesc> bprep;
     for (auto& r : rq) {
@@ -1021,12 +1039,11 @@ void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, co
       bprep.push_back(pd);
       r.src = PrepDesc{};
       r.src.src = c.wd; r.src.src_scale = 1.0;
+      r.presplit = true;
     }
-    // first pass assembles b (FP64 copy in wd) and its slices; the generic
-    // solve then re-reads b from wd for the residual
+    // b is assembled once (FP64 copy in wd for the correction residual, BF16
+    // slices for the first solve)
     add_prep(pp, P, bprep, st);
-    // pass 0 GEMMs (reuse the generic builder with the source already split):
-    // build_solves re-splits wd in pass 0, which is the same data.
     build_solves(pp, P, rq, st);
   }
 }
@@ -1037,11 +1054,15 @@ void build_precision_vort2flux(PrecisionPlan* pp, Prog& P, const DevCase* dcases
   for (auto& c : cs) { Lmax = std::max(Lmax, c.L); mns = std::max(mns, c.ns); mnq = std::max(mnq, c.nq); }
   for (int k = 2; k <= Lmax; k++) {
     std::vector<LevelItem> it;
-    for (size_t i = 0; i < cs.size(); i++) if (cs[i].L >= k) it.push_back({ids[i], k});
+    std::vector<int> cnt;
+    for (size_t i = 0; i < cs.size(); i++)
+      if (cs[i].L >= k) { it.push_back({ids[i], k}); cnt.push_back(coarsify_count(cs[i].m, cs[i].n)); }
     if (it.empty()) continue;
     LevelItem* d = upload(pp, it);
-    int ni = (int)it.size();
-    P.push_back({[=]() { launch_coarsify(dcases, d, ni, mns, st); }, TAG_STENCIL, 0.0});
+    const std::vector<int2> bmv = block_map(cnt);
+    const int2* bm = upload(pp, bmv);
+    const int nbm = (int)bmv.size();
+    P.push_back({[=]() { launch_coarsify(dcases, d, bm, nbm, st); }, TAG_STENCIL, 0.0});
   }
   for (int t = 0; t < Lmax; t++) {
     std::vector<SolveReq> rq;
@@ -1059,11 +1080,14 @@ void build_precision_vort2flux(PrecisionPlan* pp, Prog& P, const DevCase* dcases
     build_solves(pp, P, rq, st);
   }
   std::vector<LevelItem> ci;
+  std::vector<int> cnt;
   for (size_t i = 0; i < cs.size(); i++)
-    for (int k = 1; k <= (curl_all ? cs[i].L : 1); k++) ci.push_back({ids[i], k});
+    for (int k = 1; k <= (curl_all ? cs[i].L : 1); k++) { ci.push_back({ids[i], k}); cnt.push_back(cs[i].nq); }
   LevelItem* d = upload(pp, ci);
-  int ni = (int)ci.size();
-  P.push_back({[=]() { launch_curl(dcases, d, ni, mnq, st); }, TAG_STENCIL, 0.0});
+  const std::vector<int2> bmv = block_map(cnt);
+  const int2* bm = upload(pp, bmv);
+  const int nbm = (int)bmv.size();
+  P.push_back({[=]() { launch_curl(dcases, d, bm, nbm, st); }, TAG_STENCIL, 0.0});
 }
 
 void build_precision_ainv(PrecisionPlan* pp, Prog& P, const DevCase* dcases, const std::vector<DevCase>& cs,

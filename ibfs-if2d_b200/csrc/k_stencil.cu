@@ -49,12 +49,8 @@ __device__ __forceinline__ double uavg_at(const double* __restrict__ q, const do
   return 0.5 * (q[a] + q[b] + q0[a] + q0[b]);
 }
 
-__global__ void k_rhs(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items, int first_step) {
-  LevelItem it = items[blockIdx.y];
-  const DevCase& C = cases[it.c];
+__device__ __forceinline__ void rhs_at(const DevCase& C, LevelItem it, int t, int first_step) {
   int m = C.m, n = C.n;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= C.ns) return;
   int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
   int k = it.k;
   const double* om = C.omega + (size_t)(k - 1) * C.ns;
@@ -105,15 +101,23 @@ __global__ void k_rhs(const DevCase* __restrict__ cases, const LevelItem* __rest
   ro[t] = rhs;
 }
 
+// Grouped launches use a block map: block b covers elements
+// [map[b].y, map[b].y + kBlockElems) of item map[b].x, so no block is spent on
+// the parts of the grid a smaller case does not have.
+__global__ void __launch_bounds__(256) k_rhs(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items,
+                                             const int2* __restrict__ bmap, int first_step) {
+  const int2 bm = bmap[blockIdx.x];
+  const LevelItem it = items[bm.x];
+  const DevCase& C = cases[it.c];
+  const int tend = min(C.ns, bm.y + kBlockElems);
+  for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) rhs_at(C, it, t, first_step);
+}
+
 // ---------------------------------------------------------------------------
 // coarsify (operators.f90:307-333), in place on level k from level k-1.
-__global__ void k_coarsify(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items) {
-  LevelItem it = items[blockIdx.y];
-  const DevCase& C = cases[it.c];
+__device__ __forceinline__ void coarsify_at(const DevCase& C, LevelItem it, int t) {
   int m = C.m, n = C.n;
-  int ci = 3 * m / 4 - (m / 4 + 2) + 1, cj = 3 * n / 4 - (n / 4 + 2) + 1;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ci * cj) return;
+  int ci = 3 * m / 4 - (m / 4 + 2) + 1;
   int i = t % ci + m / 4 + 2, j = t / ci + n / 4 + 2;
   int ii = 2 * i - m / 2 - 1, jj = 2 * j - n / 2 - 1;
   const double* f = C.omega + (size_t)(it.k - 2) * C.ns;
@@ -123,15 +127,20 @@ __global__ void k_coarsify(const DevCase* __restrict__ cases, const LevelItem* _
                      0.25 * (R(ii - 1, jj - 1) + R(ii - 1, jj + 1) + R(ii + 1, jj - 1) + R(ii + 1, jj + 1));
 }
 
+__global__ void __launch_bounds__(256) k_coarsify(const DevCase* __restrict__ cases,
+                                                  const LevelItem* __restrict__ items, const int2* __restrict__ bmap) {
+  const int2 bm = bmap[blockIdx.x];
+  const LevelItem it = items[bm.x];
+  const DevCase& C = cases[it.c];
+  const int tend = min(coarsify_count(C.m, C.n), bm.y + kBlockElems);
+  for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) coarsify_at(C, it, t);
+}
+
 // ---------------------------------------------------------------------------
 // curl (operators.f90:243-288) of s_k with sbc_k = get_bc(s_{k+1}, 1.0)
 // (operators.f90:231; zero on the coarsest level, :218) into q_k.
-__global__ void k_curl(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items) {
-  LevelItem it = items[blockIdx.y];
-  const DevCase& C = cases[it.c];
+__device__ __forceinline__ void curl_at(const DevCase& C, LevelItem it, int t) {
   int m = C.m, n = C.n;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= C.nq) return;
   int k = it.k;
   const double* x = C.s + (size_t)(k - 1) * C.ns;
   const double* cs = (k < C.L) ? C.s + (size_t)k * C.ns : nullptr;
@@ -155,6 +164,15 @@ __global__ void k_curl(const DevCase* __restrict__ cases, const LevelItem* __res
     else v = x[nidx(i, j, m)] - x[nidx(i + 1, j, m)];
   }
   C.q[(size_t)(k - 1) * C.nq + t] = v;
+}
+
+__global__ void __launch_bounds__(256) k_curl(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items,
+                                              const int2* __restrict__ bmap) {
+  const int2 bm = bmap[blockIdx.x];
+  const LevelItem it = items[bm.x];
+  const DevCase& C = cases[it.c];
+  const int tend = min(C.nq, bm.y + kBlockElems);
+  for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) curl_at(C, it, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -184,16 +202,21 @@ __device__ __forceinline__ double reg_face(const DevCase& C, const double* __res
   return h;
 }
 
-__global__ void k_regrot(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
-  const DevCase& C = cases[cids[blockIdx.y]];
+__device__ __forceinline__ void regrot_at(const DevCase& C, int t) {
   int m = C.m, n = C.n;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= C.ns) return;
   int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
   const double* f = C.fb;
   double r = reg_face(C, f, voff(i, j, m, n)) - reg_face(C, f, voff(i - 1, j, m, n)) - reg_face(C, f, uoff(i, j, m)) +
              reg_face(C, f, uoff(i, j - 1, m));
   C.vort[t] = r;
+}
+
+__global__ void __launch_bounds__(256) k_regrot(const DevCase* __restrict__ cases, const int* __restrict__ cids,
+                                                const int2* __restrict__ bmap) {
+  const int2 bm = bmap[blockIdx.x];
+  const DevCase& C = cases[cids[bm.x]];
+  const int tend = min(C.ns, bm.y + kBlockElems);
+  for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) regrot_at(C, t);
 }
 
 // regT (operators.f90:531-546) of one face field, gathered per force in the
@@ -316,25 +339,28 @@ void launch_lastbc(const DevCase* cases, const LevelItem* items, int nitems, int
   dim3 g((max_ring + 255) / 256, nitems);
   k_lastbc<<<g, 256, 0, st>>>(cases, items);
 }
-void launch_rhs(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, int first, cudaStream_t st) {
-  if (nitems == 0) return;
-  dim3 g((max_ns + 255) / 256, nitems);
-  k_rhs<<<g, 256, 0, st>>>(cases, items, first);
+std::vector<int2> block_map(const std::vector<int>& counts) {
+  std::vector<int2> m;
+  for (int i = 0; i < (int)counts.size(); i++)
+    for (int f = 0; f < counts[i]; f += kBlockElems) m.push_back(make_int2(i, f));
+  return m;
 }
-void launch_coarsify(const DevCase* cases, const LevelItem* items, int nitems, int max_ns, cudaStream_t st) {
-  if (nitems == 0) return;
-  dim3 g((max_ns / 4 + 255) / 256 + 1, nitems);
-  k_coarsify<<<g, 256, 0, st>>>(cases, items);
+void launch_rhs(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, int first,
+                cudaStream_t st) {
+  if (nblocks == 0) return;
+  k_rhs<<<nblocks, 256, 0, st>>>(cases, items, bmap, first);
 }
-void launch_curl(const DevCase* cases, const LevelItem* items, int nitems, int max_nq, cudaStream_t st) {
-  if (nitems == 0) return;
-  dim3 g((max_nq + 255) / 256, nitems);
-  k_curl<<<g, 256, 0, st>>>(cases, items);
+void launch_coarsify(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, cudaStream_t st) {
+  if (nblocks == 0) return;
+  k_coarsify<<<nblocks, 256, 0, st>>>(cases, items, bmap);
 }
-void launch_regrot(const DevCase* cases, const int* cids, int ncases, int max_ns, cudaStream_t st) {
-  if (ncases == 0) return;
-  dim3 g((max_ns + 255) / 256, ncases);
-  k_regrot<<<g, 256, 0, st>>>(cases, cids);
+void launch_curl(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, cudaStream_t st) {
+  if (nblocks == 0) return;
+  k_curl<<<nblocks, 256, 0, st>>>(cases, items, bmap);
+}
+void launch_regrot(const DevCase* cases, const int* cids, const int2* bmap, int nblocks, cudaStream_t st) {
+  if (nblocks == 0) return;
+  k_regrot<<<nblocks, 256, 0, st>>>(cases, cids, bmap);
 }
 void launch_rhsf(const DevCase* cases, const int* cids, int ncases, int max_nf, cudaStream_t st) {
   if (ncases == 0) return;
