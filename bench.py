@@ -1,28 +1,42 @@
 #!/usr/bin/env python
 """Benchmark of the B200 IBFS per-timestep advance (one JSON line on rank 0).
 
-Workload (N=1): flat plate of chord 1 at 30 deg angle of attack, Re=300,
-400x400 cells per level, 5 nested levels, dt=0.002, domain [-2,2]^2, body
-points at spacing dx along the chord (101 points), stationary body with the
-Cholesky force solve -- seeded synthetic input of that shape (the reference
-runs no public dataset). A "step" is one full advance (operators.f90:62-188)
-of that case. The unit is cell-updates/s: L*m*n cells advanced per step.
+Metric: cell-updates/s (one cell of one level advanced one timestep; L*m*n per
+case-step) of the plain FP64 GPU advance and of the batched split-precision
+advance at <= 1e-8 relative force error, plus the cost of the discrete adjoint
+relative to a forward solve.
 
-Timing: W untimed warm-up steps, then K steps, each preceded by an L2 flush
-(a 256 MB device write; the case state is ~60 MB and would otherwise stay in
-the 126 MB L2), each timed with CUDA events on the library's stream. `value`
-is the device-timed throughput with the state resident in HBM; `e2e` is the
-same metric through the public per-step call (ibfs_advance) with the body
-velocities copied host->device from pinned memory and the forces / circulation
-/ slip copied back every step, timed on the host clock.
+Default workload (--form batch, the headline `value`): 256 independent
+stationary cases advanced together, grids drawn from {128,192,256,384,512}^2
+with 2-5 nested levels, Re log-uniform in [50,500], cylinder (D=1) or flat
+plate (chord 1, angle of attack in [0,40] deg) with body-point spacing ~dx,
+dt at CFL 0.4, FP64 Cholesky force solve per case, seed 20261203 -- seeded
+synthetic cases of those shapes (the reference runs no public dataset). A
+"step" is one advance (operators.f90:62-188) of all 256 cases: one replay of
+the captured step graph, every sine transform a split-BF16 tcgen05 GEMM plus
+one FP64 refinement sweep.
 
-`--impl reference` times the CPU restatement of the reference (the oracle,
-a port: the Fortran+FFTW reference cannot be built here) on all host cores,
-one independent case per process, on the same workload.
+Timing: W untimed warm-up steps, then K steps timed with CUDA events on the
+library's stream (ibfs_last_timing). The resident state is ~9 GB, far above
+the 126 MB L2, so no flush is needed between steps. `e2e` is the same metric
+through the public per-step call ibfs_batch_advance with host buffers: every
+step copies all cases' body velocities host->device and the step's outputs
+(forces, circulation, slip) device->host, timed on the host clock.
 
-With torchrun (N>1) every rank runs an independent replica of the case
-("replicas only": the path has no exchange step); value is the sum over ranks
-of the cell-updates divided by the max over ranks of the device time.
+Beside the headline (N=1 only): the plain FP64 advance on the 400x400x5 flat
+plate at 30 deg (Re 300, dt 0.002; L2 flushed between steps) and its ratio to
+the headline, the batched FP64 advance of the same 256 cases, the split-vs-FP64
+force and field errors, a sequential sample (cases one handle at a time), the
+split-precision plate, and the adjoint/forward cost on the rotating cylinder
+(Re 150, 256x256x4, 126 points).
+
+`--impl reference` times the CPU restatement of the reference (the oracle, a
+port: the Fortran+FFTW reference cannot be built here) on all host cores, one
+independent case per process, on a bounded sample of the same batch.
+
+With torchrun (N>1) every rank advances its own copy of the batch ("replicas
+only": the path has no exchange step); value is the sum over ranks of the
+cell-updates divided by the max over ranks of the device time.
 """
 import argparse
 import json
@@ -39,23 +53,16 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "ibfs-if2d_b200"))
 
+import workloads as W  # noqa: E402
+
 METRIC = "cell-updates/s plain vs batched split-prec at ≤1e-8 force err; adjoint/fwd cost"
 UNIT = "cell-updates/s"
-WORKLOAD = dict(workload="flat plate 30deg, Re 300, 400x400 cells x 5 levels, dt 0.002, 101 body points",
-                m=400, n=400, levels=5, re=300.0, dt=0.002, body="plate", aoa_deg=30.0, chord=1.0,
-                domain="[-2,2]^2")
-
-
-def plate_points(m, length=4.0, chord=1.0, aoa=30.0):
-    """line() of the reference geometry primitives (grid.f90:431-462)."""
-    pi = 3.1415926535897932384
-    ds = length / m
-    angle = -aoa * pi / 180.0
-    npt = int(chord / ds)
-    seg = np.arange(npt + 1, dtype=np.float64) * chord / float(npt)
-    xb = -0.5 * chord * math.cos(angle) + seg * math.cos(angle)
-    yb = -0.5 * chord * math.sin(angle) + seg * math.sin(angle)
-    return xb, yb
+SEED = 20261203
+BATCH = dict(workload="256 independent stationary cases, m in {128,192,256,384,512}, 2-5 levels, "
+                      "Re log-uniform [50,500], cylinder or plate (AoA U[0,40] deg), ds~dx, dt at CFL 0.4",
+             ncases=256, seed=SEED)
+PLATE = dict(workload="flat plate 30 deg, Re 300, 400x400 cells x 5 levels, dt 0.002, 101 body points",
+             m=400, levels=5, re=300.0, dt=0.002)
 
 
 class ClockSampler:
@@ -120,6 +127,165 @@ def dist_setup():
     return ws, rank, local
 
 
+def peaks():
+    try:
+        p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return p, "of measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "of fallback"
+
+
+def force_hist(g, hist, ncase):
+    fx = np.array([[g.outputs_of(hist[s], i)["fx"][0] for s in range(hist.shape[0])] for i in range(ncase)])
+    fy = np.array([[g.outputs_of(hist[s], i)["fy"][0] for s in range(hist.shape[0])] for i in range(ncase)])
+    return fx, fy
+
+
+def force_err(fx1, fy1, fx0, fy0):
+    """Per case max |delta Cd|, |delta Cl| over the history, relative to max |Cd|."""
+    e = [max(np.abs(fx1[i] - fx0[i]).max(), np.abs(fy1[i] - fy0[i]).max()) / np.abs(fx0[i]).max()
+         for i in range(fx0.shape[0])]
+    return float(max(e)), float(np.median(e))
+
+
+def roofline_gemm(prof, K_flops_issued, pk, src):
+    """tcgen05 GEMM class: algorithmic DST-as-GEMM flops (2 M N K per GEMM,
+    unpadded, one product) per launch / average launch time, against the
+    sustained dense BF16 peak (the kernel runs inside a long step)."""
+    d = prof["gemm_tc"]
+    if d["launches"] == 0 or d["ms"] <= 0:
+        return None
+    ach = d["flops"] / (d["ms"] / 1e3) / 1e12
+    peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+    roof = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "traffic": None, "kernel": "k_gemm_tc_persist (split-BF16 tcgen05 sine-transform GEMM)",
+            "peak_source": f"{src} (bf16 sustained)",
+            "launches_per_step": d["launches"], "avg_launch_us": d["ms"] / d["launches"] * 1e3,
+            "algorithmic_flops_per_launch": d["flops"] / d["launches"],
+            "issued_tflops": K_flops_issued / (d["ms"] / 1e3) / 1e12 if K_flops_issued else None,
+            "share_of_step": d["ms"] / sum(v["ms"] for v in prof.values())}
+    tr = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr):
+        try:
+            t = json.load(open(tr)).get("k_gemm_tc_persist_batch256")
+            if t:
+                roof["traffic"] = t["bytes_per_launch"]
+                roof["traffic_note"] = t.get("note")
+        except (OSError, ValueError):
+            pass
+    return roof
+
+
+def issued_tensor_flops(cases, nlev):
+    """Slice products actually issued per step by the split form: every solve
+    is 4 GEMMs of 6 products (first pass) + 4 of 3 (correction), on 128-row
+    and 128-column padded tiles with K padded to 64; 3L+1 solves per case."""
+    rup = lambda x, a: (x + a - 1) // a * a
+    tot = 0.0
+    for c, L in zip(cases, nlev):
+        N = c["m"] - 1
+        tot += (3 * L + 1) * 4 * 2.0 * rup(N, 128) ** 2 * rup(N, 64) * (6 + 3)
+    return tot
+
+
+def cpu_sample_from_gpu(g, cases, ids, steps):
+    """The oracle (CPU restatement, one host core) on a bounded sample of the
+    batch: the given cases, started from the GPU's state and Cholesky factor."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cells, secs = 0, 0.0
+    for i in ids:
+        c = cases[i]
+        L = g.sizes[i]["nlev"]
+        oc = O.Case(O.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"], istart=1), c["xb"], c["yb"])
+        cm, cv = g.get_cholesky(i)
+        oc.set_cholesky(cm, cv)
+        st = g.get_state(i)
+        oc.set_state(**{k: np.ascontiguousarray(v) for k, v in st.items()})
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            oc.advance()
+        secs += time.perf_counter() - t0
+        cells += L * c["m"] * c["n"] * steps
+    return {"value": cells / secs, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{len(ids)} cases of the batch (ids {ids}) x {steps} steps each on 1 host core "
+                      f"(oracle/ibfs_oracle.c, own FFT DST-I), from the GPU's state and factor; {secs:.1f} s"}
+
+
+def plain_and_split_plate(C, torch, steps, warmup, flush):
+    """Plain FP64 advance of the 400x400x5 plate (the comparison point of the
+    metric), and the split-precision form of the same case with its Cd/Cl and
+    per-level vorticity errors against FP64 over a fixed horizon."""
+    c = W.plate_re300()
+    params, bodies, _ = W.solver_args([c], C, 0)
+    out = {}
+    hs = {}
+    for prec in (0, 1):
+        g = C.Solver(params[0], bodies[0], C.make_options(precision=prec))
+        g.precompute()
+        nlev_plate = g.sizes[0]["nlev"]
+        cells = nlev_plate * c["m"] * c["n"]
+        horizon = 40
+        hs[prec] = (g.advance_n(horizon), g.get_state())
+        times = []
+        for s in range(warmup + steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            g.advance_n(1, want_hist=False)
+            if s >= warmup:
+                times.append(g.last_ms())
+        ms = sum(times) / len(times)
+        out[prec] = {"value": cells / (ms / 1e3), "ms_per_step": ms, "cells_per_step": cells,
+                     "kernels_per_step": g.kernels_per_step(), "profile_step": g.profile_step()}
+        g.close()
+    (h0, s0), (h1, s1) = hs[0], hs[1]
+    fx0, fy0 = h0[:, 0], h0[:, 1]
+    fx1, fy1 = h1[:, 0], h1[:, 1]
+    cd = np.abs(fx0).max()
+    L = nlev_plate
+    om0, om1 = s0["omega"].reshape(L, -1), s1["omega"].reshape(L, -1)  # omega(2:m,2:n,L), level slowest
+    per_level = [float(np.abs(om1[k] - om0[k]).max() / np.abs(om0[k]).max()) for k in range(L)]
+    plain = dict(out[0], workload=PLATE["workload"], form="plain FP64",
+                 l2="flushed between timed steps (256 MB write)")
+    split = dict(out[1], workload=PLATE["workload"], form="split-precision (single case)",
+                 err_vs_fp64={"steps": 40, "cd_rel_max": float(np.abs(fx1 - fx0).max() / cd),
+                              "cl_rel_to_max_cd": float(np.abs(fy1 - fy0).max() / cd),
+                              "omega_rel_max_per_level": per_level})
+    return plain, split
+
+
+def adjoint_cost(C, steps=100, K=50):
+    """Rotating cylinder (Re 150, 256x256x4, 126 points, dt .004): the discrete
+    adjoint of the mean lift over the last third of the horizon w.r.t. the
+    126 tangential surface velocities (seeded N(0, 0.1^2)); cost = device time
+    of the whole gradient run / device time of a plain forward run."""
+    m, lev, dt, re = 256, 4, 0.004, 150.0
+    xb, yb = W.circle(4.0 / m, 1.0, 0.0, 0.0, npt=126)
+    th = np.arctan2(yb, xb)
+    u = np.random.default_rng(SEED).normal(0.0, 0.1, 126)
+    vel = np.concatenate([-u * np.sin(th), u * np.cos(th)])
+    p = C.make_params(m, m, dt, re, lev)
+    f = C.Solver(p, (xb, yb))
+    f.precompute()
+    f.advance(body_vel=vel)  # the velocities stay in force for advance_n
+    f.advance_n(steps, want_hist=False)
+    ms_plain = f.last_ms()
+    cm, cv = f.get_cholesky()
+    f.close()
+    g = C.Solver(p, (xb, yb))
+    g.set_cholesky(cm, cv)
+    wx = np.zeros(steps)
+    wy = np.zeros(steps)
+    wy[-steps // 3:] = 1.0 / (steps // 3)
+    J, gv, mf, mt = g.adjoint_run(steps, K, vel, wx, wy)
+    g.close()
+    return {"cost_ratio": mt / ms_plain, "cost_ratio_vs_own_forward_pass": mt / mf, "ms_total": mt,
+            "ms_forward_pass": mf, "ms_plain_forward": ms_plain, "steps": steps, "checkpoint_every": K,
+            "workload": "rotating cylinder Re 150, 256x256 cells x 4 levels, 126 points, dt 0.004, "
+                        f"J = mean lift over the last {steps // 3} steps, grad w.r.t. 126 tangential velocities",
+            "grad_norm": float(np.linalg.norm(gv))}
+
+
 def run_ours(args):
     import torch
     import ibfs_capi as C
@@ -130,164 +296,176 @@ def run_ours(args):
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
-    W = WORKLOAD
-    xb, yb = plate_points(W["m"])
-    prec = 1 if args.form == "precision" else 0
-    params = C.make_params(W["m"], W["n"], W["dt"], W["re"], W["levels"])
-    g = C.Solver(params, (xb, yb), C.make_options(precision=prec))
+    pk, src = peaks()
+    cases = W.batch(BATCH["ncases"], seed=SEED)
+    params, bodies, opts = W.solver_args(cases, C, 1)
+    t0 = time.perf_counter()
+    g = C.Solver(params, bodies, opts)
+    t_create = time.perf_counter() - t0
+    t0 = time.perf_counter()
     g.precompute()
-    s = g.sizes[0]
-    cells = s["nlev"] * W["m"] * W["n"]
-    nf = s["nf"]
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-    def one_step():
-        flush.zero_()
-        torch.cuda.synchronize()
-        g.advance_n(1, want_hist=False)
-        return g.last_ms()
+    t_pre = time.perf_counter() - t0
+    nlev = [s["nlev"] for s in g.sizes]
+    cells = W.cells_per_step(cases, nlev)
+    ncase = len(cases)
+    nerr = 13  # force-history horizon of the error check (part of the warm-up)
 
     with ClockSampler(local) as cs:
-        # warm-up steps; keep warming until the clock sampler has a sample, so
-        # the record covers the timed region even when it is shorter than the
-        # 200 ms sampling period
+        hist_split = g.advance_n(nerr)  # warm-up steps 1..13, recorded
+        st_split = {i: g.get_state(i) for i in (0, 1, 2, 3)} if ws == 1 else None
         t_end = time.time() + 5.0
-        nw = 0
-        while nw < args.warmup or (cs.count() < 1 and time.time() < t_end):
-            one_step()
+        nw = nerr
+        while nw < args.warmup + nerr or (cs.count() < 1 and time.time() < t_end):
+            g.advance_n(1, want_hist=False)
             nw += 1
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
-        times = [one_step() for _ in range(args.steps)]
+        torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed steps
+        g.advance_n(args.steps, want_hist=False)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        tot_ms = g.last_ms()
         time.sleep(0.25)
-    tot_ms = sum(times)
     if pg:
         t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         tot_ms = float(t.item())
-        pg.barrier()
     value = cells * args.steps * ws / (tot_ms / 1e3)
     ms_per_step = tot_ms / args.steps
-
-    # per-class device time of one step (CUDA events around every launch)
-    prof = g.profile_step()
     kern = g.kernels_per_step()
 
+    # end to end through the public per-step call, host buffers
+    sum_nf = sum(s["nf"] for s in g.sizes)
+    bvel = np.zeros(sum_nf)
+    row = np.zeros(g.stride)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    te = time.perf_counter()
+    for _ in range(args.steps):
+        g.batch_advance(bvel, out=row)
+    te = time.perf_counter() - te
+    if pg:
+        t = torch.tensor([te], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        te = float(t.item())
+    e2e = {"value": cells * args.steps * ws / te, "unit": UNIT, "h2d_bytes_per_step": 8 * sum_nf,
+           "d2h_bytes_per_step": 8 * g.stride, "call": "ibfs_batch_advance", "ms_per_step": te / args.steps * 1e3}
+
+    prof = g.profile_step()  # one more step, CUDA events around every launch
     out = None
     if rank == 0:
-        # roofline of the dominant kernel class
-        dom = max(prof, key=lambda k: prof[k]["ms"])
-        peaks = {}
-        try:
-            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        except OSError:
-            pass
-        hbm = peaks.get("hbm_gbs", 6650.0)
-        bf16 = peaks.get("bf16_tflops", 1590.0)
-        peak_src = "of measured" if peaks else "of fallback"
-        step_bytes = 64.0 * cells + 8.0 * nf * nf
-        if dom in ("gemm_tc",):
-            ach = prof[dom]["flops"] / (prof[dom]["ms"] / 1e3) / 1e12
-            roof = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
-                    "traffic": None, "kernel": "tcgen05 split-BF16 sine-transform GEMM", "peak_source": peak_src}
-        elif dom == "gemm_f64":
-            # FP64 DFMA GEMM: no FP64 peak is measured on this pool; report its
-            # algorithmic rate and the whole step against the HBM roofline.
-            ach = step_bytes / (ms_per_step / 1e3) / 1e9
-            roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                    "traffic": None, "kernel": "whole step (64 B/cell-update + 8 Nf^2 B)",
-                    "peak_source": peak_src,
-                    "dominant_kernel": "k_gemm_f64 (FP64 DFMA sine-transform GEMM)",
-                    "dominant_fp64_tflops": prof[dom]["flops"] / (prof[dom]["ms"] / 1e3) / 1e12,
-                    "dominant_share": prof[dom]["ms"] / sum(v["ms"] for v in prof.values())}
-        else:
-            ach = step_bytes / (ms_per_step / 1e3) / 1e9
-            roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                    "traffic": None, "kernel": dom, "peak_source": peak_src}
-        tr = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tr):
-            try:
-                roof["traffic"] = json.load(open(tr)).get(roof.get("kernel_key", dom))
-            except (OSError, ValueError):
-                pass
-
-        e2e = None
+        roof = roofline_gemm(prof, issued_tensor_flops(cases, nlev), pk, src)
+        step_bytes = 64.0 * cells + sum(8.0 * s["nf"] ** 2 for s in g.sizes)
+        hb = step_bytes / (ms_per_step / 1e3) / 1e9
+        roof_step = {"bound": "hbm", "achieved": hb, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": hb / pk["hbm_gbs"], "peak_source": src,
+                     "basis": "whole step: 64 B per cell-update + 8 Nf^2 B per case"}
+        extras = {}
         cpu = None
-        if ws == 1:
-            # end to end through the public per-step call, host buffers
-            import ctypes
-            vel = np.zeros(nf)
-            hv = torch.zeros(nf, dtype=torch.float64).pin_memory()
-            e2e_s = 0.0
-            for _ in range(args.steps):
-                flush.zero_()
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                vel[:] = hv.numpy()
-                o = g.advance(body_vel=vel)
-                e2e_s += time.perf_counter() - t0
-            d2h = 8 * (2 * s["nbody"] + s["nlev"] + 1)
-            e2e = {"value": cells * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * nf,
-                   "d2h_bytes_per_step": d2h}
-            # CPU baseline: the oracle on one host core, from the GPU's state
-            cpu = cpu_baseline_sample(g, params, xb, yb, cells, args.cpu_steps)
-
+        if ws == 1 and not args.no_extras:
+            # batched FP64 on the same cases, same factor; force error of the split form
+            p0, b0, o0 = W.solver_args(cases, C, 0)
+            f = C.Solver(p0, b0, o0)
+            for i in range(ncase):
+                f.set_cholesky(*g.get_cholesky(i), icase=i)
+            hist_f = f.advance_n(nerr)
+            fx0, fy0 = force_hist(f, hist_f, ncase)
+            fx1, fy1 = force_hist(g, hist_split, ncase)
+            emax, emed = force_err(fx1, fy1, fx0, fy0)
+            ferr = {}
+            for i in st_split:
+                a, b = st_split[i]["omega"], f.get_state(i)["omega"]
+                ferr[str(i)] = float(np.abs(a - b).max() / np.abs(b).max())
+            f.advance_n(args.warmup, want_hist=False)
+            f.advance_n(5, want_hist=False)
+            fms = f.last_ms() / 5
+            extras["batched_fp64"] = {"value": cells / (fms / 1e3), "ms_per_step": fms,
+                                      "kernels_per_step": f.kernels_per_step()}
+            f.close()
+            extras["force_err_vs_fp64"] = {"max": emax, "median": emed, "steps": nerr, "cases": ncase,
+                                           "basis": "max over the history of |dCd|,|dCl| / max|Cd|, per case; "
+                                                    "reference = the batched FP64 GPU advance (within 1e-10 "
+                                                    "of the oracle)"}
+            extras["omega_err_vs_fp64"] = {"cases": ferr, "steps": nerr, "basis": "max |d omega| / max |omega|"}
+            # sequential sample: cases advanced one handle at a time
+            rng = np.random.default_rng(SEED + 1)
+            ids = sorted(int(x) for x in rng.choice(ncase, 16, replace=False))
+            sc, sms = 0, 0.0
+            for i in ids:
+                s = C.Solver(params[i], bodies[i], opts[i])
+                s.set_cholesky(*g.get_cholesky(i))
+                s.advance_n(2, want_hist=False)
+                s.advance_n(3, want_hist=False)
+                sms += s.last_ms() / 3
+                sc += nlev[i] * cases[i]["m"] * cases[i]["n"]
+                s.close()
+            extras["sequential_sample"] = {"value": sc / (sms / 1e3), "cases": ids, "form": "split-precision",
+                                           "basis": "sum of cells / sum of per-case device step times"}
+            flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+            plain, split = plain_and_split_plate(C, torch, args.steps, args.warmup, flush)
+            extras["plain_fp64"] = plain
+            extras["ratio_vs_plain_fp64"] = value / plain["value"]
+            extras["plate400_split"] = split
+            extras["adjoint"] = adjoint_cost(C)
+            cpu = cpu_sample_from_gpu(g, cases, sorted(int(x) for x in np.random.default_rng(SEED + 2).choice(
+                ncase, 6, replace=False)), args.cpu_steps)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == 0 else "bf16x3+f64",
-            "data": "synthetic (seeded geometry of the named config; no dataset)",
-            "config": dict(WORKLOAD, form="plain FP64" if prec == 0 else "split-precision",
-                           l2="flushed between timed steps (256 MB write)",
-                           parallelism="replicas" if ws > 1 else "single GPU"),
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kern * args.steps,
-            "kernels_per_step": kern, "profile_step": prof, "clocks": cs.summary(),
-            "impl": "ours",
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3+f64",
+            "data": "synthetic (seeded cases of the named shapes; no dataset)",
+            "config": dict(BATCH, cells_per_step=cells, form="batched split-precision",
+                           l2="inputs larger than L2 (~9 GB resident state), no flush",
+                           parallelism="replicas" if ws > 1 else "single GPU",
+                           create_s=t_create, precompute_s=t_pre),
+            "roofline": roof, "roofline_step_hbm": roof_step, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": kern * args.steps, "kernels_per_step": kern, "profile_step": prof,
+            "clocks": cs.summary(), "impl": "ours",
         }
+        out.update(extras)
         print(json.dumps(out), flush=True)
+    g.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
     return out
 
 
-def cpu_baseline_sample(g, params, xb, yb, cells, steps):
-    """Time the oracle (CPU restatement, one core) on a bounded sample of the
-    same workload, started from the GPU's current state and Cholesky factor."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    p = O.make_params(params.m, params.n, params.dt, params.re, params.mgridlev, istart=1)
-    c = O.Case(p, xb, yb)
-    cm, cv = g.get_cholesky()
-    c.set_cholesky(cm, cv)
-    st = g.get_state()
-    c.set_state(**{k: np.ascontiguousarray(v) for k, v in st.items()})
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        c.advance()
-    dt = time.perf_counter() - t0
-    return {"value": cells * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{steps} steps of the same case on 1 host core (oracle/ibfs_oracle.c, own FFT DST-I), "
-                      f"from the GPU's state; {dt:.1f} s"}
+def run_single(args):
+    """--form plain / precision: the 400x400x5 plate alone (diagnostic form)."""
+    import torch
+    import ibfs_capi as C
+    pk, src = peaks()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    plain, split = plain_and_split_plate(C, torch, args.steps, args.warmup, flush)
+    d = plain if args.form == "plain" else split
+    out = {"metric": METRIC, "value": d["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": d["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64" if args.form == "plain" else "bf16x3+f64",
+           "data": "synthetic (seeded geometry of the named config; no dataset)",
+           "config": {"workload": PLATE["workload"], "form": d["form"], "l2": d["l2"] if "l2" in d else
+                      "flushed between timed steps (256 MB write)"},
+           "plain_fp64": plain, "plate400_split": split, "impl": "ours",
+           "gpu_launches": d["kernels_per_step"] * args.steps}
+    print(json.dumps(out), flush=True)
 
 
-def _ref_worker(args):
-    steps, warmup, seed = args
+def _ref_worker(a):
+    i, steps, warmup = a
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    W = WORKLOAD
-    xb, yb = plate_points(W["m"])
-    c = O.Case(O.make_params(W["m"], W["n"], W["dt"], W["re"], W["levels"]), xb, yb)
+    c = W.batch(BATCH["ncases"], seed=SEED)[i]
+    oc = O.Case(O.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"]), c["xb"], c["yb"])
     for _ in range(warmup):
-        c.advance()  # first step runs preprocess (untimed), as advance does at itime==1
+        oc.advance()  # the first step runs preprocess (untimed), as advance does at itime==1
     t0 = time.perf_counter()
     for _ in range(steps):
-        c.advance()
-    return time.perf_counter() - t0, W["levels"] * W["m"] * W["n"] * steps
+        oc.advance()
+    return time.perf_counter() - t0, oc.nlev * c["m"] * c["n"] * steps
 
 
 def run_reference(args):
@@ -298,24 +476,30 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.build()
+    cases = W.batch(BATCH["ncases"], seed=SEED)
+    small = [i for i, c in enumerate(cases) if c["m"] <= 192]
     ncores = os.cpu_count() or 1
-    procs = max(1, min(ncores, args.ref_procs))
+    procs = max(1, min(ncores, args.ref_procs, len(small)))
+    ids = small[:procs]
     steps = max(1, min(args.steps, args.ref_steps))
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(steps, max(1, args.warmup), i) for i in range(procs)])
+        res = pool.map(_ref_worker, [(i, steps, max(1, args.warmup)) for i in ids])
     tmax = max(r[0] for r in res)
     cells = sum(r[1] for r in res)
     value = cells / tmax
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": args.warmup,
         "ms_per_step": tmax / steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded geometry of the named config; no dataset)",
-        "config": dict(WORKLOAD, form="CPU restatement (oracle port)", parallelism=f"{procs} processes"),
+        "dtype": "f64", "data": "synthetic (seeded cases of the named shapes; no dataset)",
+        "config": dict(BATCH, form="CPU restatement (oracle port), one case per process",
+                       parallelism=f"{procs} processes"),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
-                         "sample": f"{procs} independent cases x {steps} steps after {max(1, args.warmup)} "
-                                   f"warm-up steps (first one runs the Cholesky preprocess)"},
+                         "sample": f"{procs} cases of the batch with m <= 192 (ids {ids[:8]}...), one per "
+                                   f"process, {steps} timed steps each after {max(1, args.warmup)} warm-up "
+                                   f"steps (the first runs the Cholesky preprocess); the Fortran+FFTW "
+                                   f"reference cannot be built here"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -328,17 +512,21 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain", "precision"])
-    ap.add_argument("--cpu-steps", type=int, default=12)
+    ap.add_argument("--form", default="batch", choices=["batch", "plain", "precision"])
+    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline batch measurement only (no FP64 / plate / adjoint / CPU legs)")
     ap.add_argument("--ref-procs", type=int, default=128)
-    ap.add_argument("--ref-steps", type=int, default=20)
+    ap.add_argument("--ref-steps", type=int, default=10)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
-    else:
+    elif args.form == "batch":
         run_ours(args)
+    else:
+        run_single(args)
 
 
 if __name__ == "__main__":

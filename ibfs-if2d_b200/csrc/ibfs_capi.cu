@@ -775,6 +775,16 @@ static int finish_create(ibfs_handle* h) {
   }
   h->out_stride = off;
   h->d_out = dalloc<double>(h, off);
+  // body velocities of all cases in one array, so that a batched step moves
+  // them with one copy
+  for (auto& c : h->cases) h->sum_nf += c.nf;
+  h->d_bvel = dalloc<double>(h, h->sum_nf);
+  if (!h->d_bvel || cudaMallocHost(&h->h_bvel, sizeof(double) * std::max(1, h->sum_nf)) != cudaSuccess)
+    return fail(IBFS_ERR_NOMEM, "body velocity buffers");
+  for (int i = 0, o = 0; i < nc; i++) {
+    h->cases[i].dc.bvel = h->d_bvel + o;
+    o += h->cases[i].nf;
+  }
   int nitems = 0;
   for (auto& c : h->cases) nitems += c.L;
   h->d_partial = dalloc<double>(h, (size_t)nitems * 32);
@@ -859,6 +869,7 @@ static void free_handle(ibfs_handle* h) {
   if (h->gx_post) cudaGraphExecDestroy(h->gx_post);
   for (void* p : h->allocs) cudaFree(p);
   if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->h_bvel) cudaFreeHost(h->h_bvel);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->st) cudaStreamDestroy(h->st);
@@ -1025,6 +1036,32 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
   if (fy) memcpy(fy, o + c.nbody, sizeof(double) * c.nbody);
   if (circ) memcpy(circ, o + 2 * c.nbody, sizeof(double) * c.L);
   if (slip) *slip = o[2 * c.nbody + c.L];
+  return IBFS_OK;
+}
+
+int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out) {
+  if (!h) return IBFS_ERR_ARG;
+  bool need = false;
+  for (auto& c : h->cases) if (c.p.stationary && !c.have_chol) need = true;
+  if (need) {
+    int rc = precompute(h);
+    if (rc) { h->err = t_error; return rc; }
+  }
+  if (body_vel) {
+    memcpy(h->h_bvel, body_vel, sizeof(double) * h->sum_nf);
+    IBFS_CUDA_CHECK(cudaMemcpyAsync(h->d_bvel, h->h_bvel, sizeof(double) * h->sum_nf, cudaMemcpyHostToDevice, h->st));
+  } else {
+    IBFS_CUDA_CHECK(cudaMemsetAsync(h->d_bvel, 0, sizeof(double) * h->sum_nf, h->st));
+  }
+  int rc = run_step(h);
+  if (rc) { h->err = t_error; return rc; }
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(h->h_stage, h->d_out, sizeof(double) * h->out_stride, cudaMemcpyDeviceToHost, h->st));
+  int status = 0;
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  if (status & 2) return fail(IBFS_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM)");
+  if (out) memcpy(out, h->h_stage, sizeof(double) * h->out_stride);
+  for (auto& c : h->cases) c.itime += 1;
   return IBFS_OK;
 }
 

@@ -73,6 +73,9 @@ struct ibfs_handle {
   int max_ns = 0, max_nq = 0, max_nf = 0, max_ring = 0, max_L = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double* h_stage = nullptr;  // pinned staging for outputs / body velocities
+  double* d_bvel = nullptr;   // every case's body velocities, contiguous in case order
+  double* h_bvel = nullptr;   // pinned staging of the same
+  int sum_nf = 0;
   AdjPlan* adj = nullptr;
 };
 

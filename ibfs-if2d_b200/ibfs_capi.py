@@ -22,7 +22,7 @@ _ERRNAMES = {1: "IBFS_ERR_GRID", 2: "IBFS_ERR_CHOL", 3: "IBFS_ERR_CG_MAXITER", 4
 EXPORTS = [
     "ibfs_create", "ibfs_batch_create", "ibfs_destroy", "ibfs_case_sizes", "ibfs_num_cases",
     "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
-    "ibfs_advance", "ibfs_advance_n", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
+    "ibfs_advance", "ibfs_advance_n", "ibfs_batch_advance", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
     "ibfs_last_cg_iterations", "ibfs_adjoint_run",
     "ibfs_last_error",
@@ -82,6 +82,7 @@ def lib():
         L.ibfs_precompute.argtypes = [vp]
         L.ibfs_advance.argtypes = [vp, _IP, _DP, _DP, _DP, _DP, _DP]
         L.ibfs_advance_n.argtypes = [vp, ctypes.c_int, _DP]
+        L.ibfs_batch_advance.argtypes = [vp, _DP, _DP]
         L.ibfs_output_offset.argtypes = [vp, ctypes.c_int]
         L.ibfs_output_stride.argtypes = [vp]
         L.ibfs_apply_op.argtypes = [vp, ctypes.c_int, _DP, _DP]
@@ -205,6 +206,19 @@ class Solver:
         self._check(lib().ibfs_advance_n(self.h, nsteps, _p(hist)))
         self.itime.value += nsteps
         return hist.reshape(nsteps, self.stride) if want_hist else None
+
+    def batch_advance(self, body_vel=None, out=None):
+        """One advance of every case (ibfs_batch_advance): body_vel = all cases'
+        body-point velocities concatenated (or None); returns the step's
+        output row (layout of one advance_n history row)."""
+        if out is None:
+            out = np.zeros(self.stride)
+        bv = None if body_vel is None else np.ascontiguousarray(body_vel, dtype=np.float64)
+        if bv is not None:
+            assert bv.size == sum(s["nf"] for s in self.sizes), "body_vel must hold every case's Nf values"
+        self._check(lib().ibfs_batch_advance(self.h, _p(bv), _p(out)))
+        self.itime.value += 1
+        return out
 
     def outputs_of(self, hist_row, icase=0):
         s = self.sizes[icase]

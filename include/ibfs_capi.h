@@ -116,9 +116,19 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
 
 /* nsteps advances of every case, replayed from one captured CUDA graph per
  * step. hist (may be NULL) receives, per step, per case, the output block
- * [fx(nbody) fy(nbody) circ(L) slip]; ibfs_output_stride gives the per-case
- * block length and ibfs_output_offset its offset within a step. */
+ * [fx(nbody) fy(nbody) circ(L) slip]; ibfs_output_stride gives the doubles
+ * of one step (all cases) and ibfs_output_offset a case's offset within it.
+ * The body velocities are those of the last ibfs_advance/ibfs_batch_advance
+ * (zero initially). */
 int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist);
+
+/* One advance of every case of a handle: the batched counterpart of
+ * ibfs_advance (the reference runs one case per process, main.f90:42-54).
+ * body_vel: every case's Nf body-point velocities in flow units, concatenated
+ * in case order (NULL = 0); they stay in force for later ibfs_advance_n calls.
+ * out (may be NULL): the step's outputs, ibfs_output_stride doubles laid out
+ * as one step of ibfs_advance_n's history. */
+int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out);
 int ibfs_output_offset(const ibfs_handle* h, int icase);
 int ibfs_output_stride(const ibfs_handle* h);
 

@@ -48,3 +48,24 @@ def test_batch_equals_single_handles():
         s = C.Solver(params[ic], bodies[ic], opts[ic])
         s.advance_n(4, want_hist=False)
         assert np.array_equal(s.get_state()["omega"], g.get_state(ic)["omega"]), ic
+
+
+def test_batch_advance_per_step_call():
+    """ibfs_batch_advance (host body velocities in, one step's outputs out)
+    reproduces advance_n's history bit for bit, and body velocities given to
+    it equal those given to single-case ibfs_advance calls."""
+    params, bodies, opts = W.solver_args(SMALL, C, 0)
+    a = C.Solver(params, bodies, opts)
+    b = C.Solver(params, bodies, opts)
+    hist = a.advance_n(3)
+    rows = [b.batch_advance() for _ in range(3)]
+    assert np.array_equal(np.array(rows), hist)
+    rng = np.random.default_rng(5)
+    vels = [0.05 * rng.standard_normal(s["nf"]) for s in b.sizes]
+    row = b.batch_advance(np.concatenate(vels))
+    for ic in range(len(SMALL)):
+        s = C.Solver(params[ic], bodies[ic], opts[ic])
+        s.advance_n(3, want_hist=False)
+        o = s.advance(body_vel=vels[ic])
+        assert np.array_equal(b.outputs_of(row, ic)["fx"], o["fx"]), ic
+        assert np.array_equal(b.get_state(ic)["omega"], s.get_state()["omega"]), ic
