@@ -1015,7 +1015,9 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
     c.itime = *itime;
     IBFS_CUDA_CHECK(cudaMemcpyAsync(h->d_itime, itime, sizeof(int), cudaMemcpyHostToDevice, h->st));
   }
-  if (*itime + 1 == 1 || !c.have_chol) {
+  // preprocess at the first step (operators.f90:88-90), unless the caller
+  // supplied the factor (the reference reads input/ibfs.chd then, :44-46)
+  if (c.p.stationary && !c.have_chol) {
     int rc = precompute(h);
     if (rc) { h->err = t_error; return rc; }
   }
@@ -1025,8 +1027,11 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
   } else {
     IBFS_CUDA_CHECK(cudaMemsetAsync(c.dc.bvel, 0, sizeof(double) * c.nf, h->st));
   }
+  // IBFS_ERR_CG_MAXITER is the reference's warning (operators.f90:435-438):
+  // the step is complete, so its outputs are still returned
   int rc = run_step(h);
-  if (rc) { h->err = t_error; return rc; }
+  if (rc && rc != IBFS_ERR_CG_MAXITER) { h->err = t_error; return rc; }
+  if (rc) h->err = t_error;
   double* o = h->h_stage + c.nf;
   IBFS_CUDA_CHECK(cudaMemcpyAsync(o, h->d_out, sizeof(double) * h->out_stride, cudaMemcpyDeviceToHost, h->st));
   IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
@@ -1036,7 +1041,7 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
   if (fy) memcpy(fy, o + c.nbody, sizeof(double) * c.nbody);
   if (circ) memcpy(circ, o + 2 * c.nbody, sizeof(double) * c.L);
   if (slip) *slip = o[2 * c.nbody + c.L];
-  return IBFS_OK;
+  return rc;
 }
 
 int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out) {
@@ -1054,7 +1059,8 @@ int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out) {
     IBFS_CUDA_CHECK(cudaMemsetAsync(h->d_bvel, 0, sizeof(double) * h->sum_nf, h->st));
   }
   int rc = run_step(h);
-  if (rc) { h->err = t_error; return rc; }
+  if (rc && rc != IBFS_ERR_CG_MAXITER) { h->err = t_error; return rc; }
+  if (rc) h->err = t_error;
   IBFS_CUDA_CHECK(cudaMemcpyAsync(h->h_stage, h->d_out, sizeof(double) * h->out_stride, cudaMemcpyDeviceToHost, h->st));
   int status = 0;
   IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
@@ -1062,7 +1068,7 @@ int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out) {
   if (status & 2) return fail(IBFS_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM)");
   if (out) memcpy(out, h->h_stage, sizeof(double) * h->out_stride);
   for (auto& c : h->cases) c.itime += 1;
-  return IBFS_OK;
+  return rc;
 }
 
 int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist) {
@@ -1080,8 +1086,10 @@ int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist) {
     h->hist_steps = nsteps;
   }
   IBFS_CUDA_CHECK(cudaEventRecord(h->ev0, h->st));
+  int warn = IBFS_OK;
   for (int s = 0; s < nsteps; s++) {
     int rc = run_step(h);
+    if (rc == IBFS_ERR_CG_MAXITER) { h->err = t_error; warn = rc; rc = IBFS_OK; }
     if (rc) { h->err = t_error; return rc; }
     if (hist)
       IBFS_CUDA_CHECK(cudaMemcpyAsync(h->d_hist + (size_t)s * h->out_stride, h->d_out,
@@ -1097,7 +1105,7 @@ int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist) {
   cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
   if (status & 2) return fail(IBFS_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM)");
   for (auto& c : h->cases) c.itime += nsteps;
-  return IBFS_OK;
+  return warn;
 }
 
 int ibfs_output_offset(const ibfs_handle* h, int icase) {

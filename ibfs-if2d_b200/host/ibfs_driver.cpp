@@ -1,0 +1,245 @@
+// ibfs_driver.cpp -- host driver of the B200 IBFS advance (program ibfs_gpu).
+//
+// The reference's PROGRAM main (main.f90:12-63) with the time step on the
+// GPU: same run directory, same input files, same output files.
+//   input      input/ibfs.inp (&READ_PARAMETERS; written with the defaults if
+//              absent, parameters.f90:54-69), optional &B200_OPTIONS group
+//   setup      input/geom.inp, or a circle of diameter 1 at the origin when it
+//              is absent (grid.f90:252-353); grid checks and regularisation
+//              happen in ibfs_create
+//   variables  istart = 0: zero (or uniform) flow; otherwise
+//              output/ibfsNNNNNNN.var and, for a stationary body,
+//              input/ibfs.chd (variables.f90:28-77)
+//   preprocess first step of a stationary body: input/ibfs.chd if present,
+//              else ibfs_precompute and write input/ibfs.chd
+//              (operators.f90:29-59)
+//   advance    ibfs_advance per step; every isave steps and at istop the
+//              restart record; force.dat / circ.dat / slip.dat every step
+//              (operators.f90:176-188, 549-699)
+// Actuator points (bodyno < 0, grid.f90:579-718) are not supported.
+//
+//   ibfs_gpu [-C dir] [--dry-run]
+// --dry-run reads and checks the inputs (and a restart record when
+// istart > 0) and prints them as JSON without touching the GPU.
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <vector>
+
+#include "ibfs_io.h"
+
+using namespace ibfs_host;
+
+namespace {
+
+FILE* g_inf = nullptr;
+
+void logline(const std::string& s) {
+  if (g_inf) {
+    std::fprintf(g_inf, " %s\n", s.c_str());
+    std::fflush(g_inf);
+  }
+}
+
+int stop(const std::string& msg, int code) {
+  std::fprintf(stderr, "%s\n", msg.c_str());
+  logline(msg);
+  if (g_inf) std::fclose(g_inf);
+  return code;
+}
+
+void append_line(const std::string& path, int it, const std::string& line) {
+  // the reference replaces the file at it == 1 and appends otherwise
+  // (creating it when missing), operators.f90:564-573
+  FILE* f = std::fopen(path.c_str(), it == 1 ? "w" : "a");
+  if (!f) return;
+  std::fprintf(f, "%s\n", line.c_str());
+  std::fclose(f);
+}
+
+std::string var_name(int it) {
+  char b[64];
+  std::snprintf(b, sizeof b, "output/ibfs%07d.var", it);
+  return b;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  bool dry = false;
+  for (int a = 1; a < argc; a++) {
+    if (!std::strcmp(argv[a], "--dry-run")) dry = true;
+    else if (!std::strcmp(argv[a], "-C") && a + 1 < argc) {
+      if (::chdir(argv[++a]) != 0) return stop(std::string("cannot enter ") + argv[a], 2);
+    } else {
+      std::fprintf(stderr, "usage: ibfs_gpu [-C dir] [--dry-run]\n");
+      return 2;
+    }
+  }
+  ::mkdir("output", 0755);
+  ::mkdir("input", 0755);
+  auto t0 = std::chrono::steady_clock::now();
+  if (!dry) {
+    g_inf = std::fopen("output/ibfs.inf", "a");
+    logline("===================================");
+    logline("|   Welcome to IBFS MGRID v1.0    |");
+    logline("|   (GPU time step, B200 build)   |");
+    logline("===================================");
+    std::time_t now = std::time(nullptr);
+    char tb[64];
+    std::strftime(tb, sizeof tb, "Executed at time: %H%M%S on date: %Y%m%d", std::localtime(&now));
+    logline(tb);
+    std::printf("\n=======================================\n|     Welcome to IBFS MGRID v1.0      |\n"
+                "|  time step on the GPU (B200 build)  |\n=======================================\n\n%s\n",
+                tb);
+  }
+
+  // INPUT (parameters.f90:54-69)
+  ibfs_params_c p = default_params();
+  ibfs_options_c opt{};
+  opt.tile_cfg = -1;
+  std::string msg;
+  if (file_exists("input/ibfs.inp")) {
+    bool ok = false;
+    std::string text = file_text("input/ibfs.inp", ok);
+    if (!ok || !parse_read_parameters(text, p, msg)) return stop("input/ibfs.inp: " + msg, 2);
+    if (!parse_b200_options(text, opt, msg)) return stop("input/ibfs.inp: " + msg, 2);
+    logline("... Read parameters from ibfs.inp");
+  } else {
+    if (FILE* f = std::fopen("input/ibfs.inp", "w")) {
+      std::fputs(format_read_parameters(p).c_str(), f);
+      std::fclose(f);
+    }
+    logline("... loading default run");
+  }
+  logline("... Input parameters follow");
+  if (g_inf) std::fputs(format_read_parameters(p).c_str(), g_inf);
+
+  // SETUP GEOMETRY (grid.f90:252-353)
+  Geometry geo;
+  if (file_exists("input/geom.inp")) {
+    if (!read_geometry("input/geom.inp", geo, msg)) return stop(msg, 2);
+    logline("Reading geometry from geom.inp");
+    if (!dry) std::printf("Reading geometry from geom.inp\n");
+  } else {
+    geo = default_geometry(p);
+  }
+  for (int b : geo.bodyno)
+    if (b < 0) return stop("actuator points (bodyno < 0) are not supported by this driver", 2);
+  const int nb = (int)geo.x.size();
+
+  if (dry) {
+    std::vector<double> var_sums;
+    if (p.istart > 0) {  // check the restart record against the grid
+      int L = p.mgridlev;  // the level clamp is applied by ibfs_create; the dry run reads the namelist value
+      size_t ns = (size_t)(p.m - 1) * (p.n - 1), nq = (size_t)(p.m + 1) * p.n + (size_t)(p.n + 1) * p.m;
+      std::vector<size_t> cnt = {ns * L, (size_t)2 * nb, ns * L, nq * L, nq * L};
+      std::vector<std::vector<double>> buf;
+      std::vector<double*> parts;
+      for (size_t c : cnt) buf.emplace_back(c);
+      for (auto& b : buf) parts.push_back(b.data());
+      if (!read_record(var_name(p.istart), parts, cnt, msg)) return stop(msg, 2);
+      for (auto& b : buf) {
+        double s = 0.0;
+        for (double v : b) s += v;
+        var_sums.push_back(s);
+      }
+    }
+    std::printf("{\"istart\": %d, \"istop\": %d, \"isave\": %d, \"m\": %d, \"n\": %d, \"dt\": %.17g, "
+                "\"re\": %.17g, \"cgtol\": %.17g, \"cg_max_iter\": %d, \"unif_flow\": %d, \"len\": %.17g, "
+                "\"offsetx\": %.17g, \"offsety\": %.17g, \"mgridlev\": %d, \"make_vortex\": %d, "
+                "\"stationary\": %d, \"precision\": %d, \"cg_relative\": %d, \"motion_kind\": %d, "
+                "\"tile_cfg\": %d, \"nb\": %d, \"x0\": %.17g, \"y0\": %.17g, \"var_sums\": [",
+                p.istart, p.istop, p.isave, p.m, p.n, p.dt, p.re, p.cgtol, p.cg_max_iter, p.unif_flow, p.len,
+                p.offsetx, p.offsety, p.mgridlev, p.make_vortex, p.stationary, opt.precision, opt.cg_relative,
+                opt.motion_kind, opt.tile_cfg, nb, nb ? geo.x[0] : 0.0, nb ? geo.y[0] : 0.0);
+    for (size_t i = 0; i < var_sums.size(); i++) std::printf("%s%.17g", i ? ", " : "", var_sums[i]);
+    std::printf("]}\n");
+    return 0;
+  }
+
+  // SETUP + SETUP_VARIABLES (grid.f90:44-139, variables.f90:28-77)
+  ibfs_handle* h = nullptr;
+  int rc = ibfs_create(&p, &opt, nb, geo.x.data(), geo.y.data(), geo.bodyno.data(), &h);
+  if (rc) return stop(std::string("ibfs_create: ") + ibfs_last_error(h), 10 + rc);
+  int m, n, L, nq, nbb, nbody;
+  ibfs_case_sizes(h, 0, &m, &n, &L, &nq, &nbb, &nbody);
+  const size_t ns = (size_t)(m - 1) * (n - 1);
+  const int nf = 2 * nbb;
+  std::vector<double> omega(ns * L), fb(nf), rhs_old(ns * L), q((size_t)nq * L), q0((size_t)nq * L);
+  std::vector<double> cholmat((size_t)nf * nf), cholvec(nf);
+  auto read_chd = [&]() -> bool {
+    if (!read_record("input/ibfs.chd", {cholmat.data(), cholvec.data()}, {cholmat.size(), cholvec.size()}, msg))
+      return false;
+    logline("Reading Cholesky decompopsition...");
+    std::printf("Reading Cholesky premade decomposition...\n");
+    return ibfs_set_cholesky(h, 0, cholmat.data(), cholvec.data()) == IBFS_OK;
+  };
+  if (p.istart > 0) {
+    if (!read_record(var_name(p.istart), {omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data()},
+                     {omega.size(), fb.size(), rhs_old.size(), q.size(), q0.size()}, msg))
+      return stop(msg, 5);
+    rc = ibfs_set_state(h, 0, omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data());
+    if (rc) return stop(std::string("ibfs_set_state: ") + ibfs_last_error(h), 10 + rc);
+    logline("Reading restart file at itime= " + std::to_string(p.istart));
+    std::printf("Reading restart file at itime = %d\n", p.istart);
+    if (p.stationary && !read_chd()) return stop("input/ibfs.chd: " + msg, 5);
+  }
+
+  // TIME MARCH (main.f90:45-50)
+  std::vector<double> fx(nbody > 0 ? nbody : 1), fy(nbody > 0 ? nbody : 1), circ(L);
+  double slip = 0.0;
+  int it = p.istart;
+  while (it < p.istop) {
+    if (it + 1 == 1 && p.stationary) {  // preprocess (operators.f90:88-90)
+      if (file_exists("input/ibfs.chd")) {
+        if (!read_chd()) return stop("input/ibfs.chd: " + msg, 5);
+      } else {
+        std::printf("Precomputing body matrix...\n");
+        logline("Precomputing body matrix...");
+        rc = ibfs_precompute(h);
+        if (rc) return stop(std::string("ibfs_precompute: ") + ibfs_last_error(h), 10 + rc);
+        ibfs_get_cholesky(h, 0, cholmat.data(), cholvec.data());
+        if (!write_record("input/ibfs.chd", {cholmat.data(), cholvec.data()}, {cholmat.size(), cholvec.size()},
+                          msg))
+          return stop(msg, 5);
+        logline("Saving cholesky decomposition...");
+      }
+    }
+    std::printf(" \n-------------------------------------------\n * For itime = %d\n", it + 1);
+    logline("...Advancing to itime = " + std::to_string(it + 1));
+    rc = ibfs_advance(h, &it, nullptr, fx.data(), fy.data(), circ.data(), &slip);
+    if (rc == IBFS_ERR_CG_MAXITER) {  // the reference warns and carries on (operators.f90:435-438)
+      logline("WARNING!! CJGR used max iterations!");
+      std::printf(" => itmax = %d\n", p.cg_max_iter);
+    } else if (rc) {
+      return stop(std::string("ibfs_advance: ") + ibfs_last_error(h), 10 + rc);
+    }
+    if (it % p.isave == 0 || it == p.istop) {  // write_variables (variables.f90:141-155)
+      ibfs_get_state(h, 0, omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data());
+      if (!write_record(var_name(it), {omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data()},
+                        {omega.size(), fb.size(), rhs_old.size(), q.size(), q0.size()}, msg))
+        return stop(msg, 5);
+      logline("Writing restart file at itime= " + std::to_string(it));
+    }
+    std::vector<double> fv;
+    for (int b = 0; b < nbody; b++) fv.push_back(fx[b]);
+    for (int b = 0; b < nbody; b++) fv.push_back(fy[b]);
+    append_line("output/force.dat", it, list_directed(it, fv));
+    logline("Computed x- & y-forces at itime= " + std::to_string(it));
+    append_line("output/circ.dat", it, list_directed(it, circ));
+    append_line("output/slip.dat", it, list_directed(it, {slip}));
+    std::printf(" SLIP = %.17g\n", slip);
+  }
+  ibfs_destroy(h);
+  double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::printf(" \n Total run time: %.6f s\n \n", secs);
+  logline("Total run time: " + std::to_string(secs) + " s");
+  if (g_inf) std::fclose(g_inf);
+  return 0;
+}

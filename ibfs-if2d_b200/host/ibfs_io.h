@@ -1,0 +1,66 @@
+// ibfs_io.h -- host-side file formats of the IBFS driver (no CUDA).
+//
+// The reference keeps all I/O in its Fortran host code; the B200 driver keeps
+// the same files so that a run directory works with either program:
+//   input/ibfs.inp   namelist &READ_PARAMETERS (parameters.f90:48-69)
+//   input/geom.inp   ntot, then "x y bodyno" per point (grid.f90:270-277)
+//   input/ibfs.chd   one unformatted record: cholmat(Nf,Nf), cholvec(Nf) (variables.f90:110-137)
+//   output/ibfsNNNNNNN.var  one unformatted record: omega, fb, rhs_old, q, q0 (variables.f90:141-175)
+//   output/force.dat, circ.dat, slip.dat  one list-directed line per step (operators.f90:549-699)
+//   output/ibfs.inf  run log (main.f90:21-29)
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ibfs_capi.h"
+
+namespace ibfs_host {
+
+// Reference defaults (parameters.f90:12-31).
+ibfs_params_c default_params();
+
+// Parses the &READ_PARAMETERS group of a namelist text into p (fields not
+// present keep their value). Names are case-insensitive; values may be
+// Fortran integers, reals (E or D exponents, trailing '.') or logicals
+// (T, F, .TRUE., .FALSE.). Returns false with msg set on a malformed group or
+// an unknown name.
+bool parse_read_parameters(const std::string& text, ibfs_params_c& p, std::string& msg);
+
+// Optional &B200_OPTIONS group of the same file (precision, cg_relative,
+// motion_kind, pitch_amp_deg, pitch_freq, pivot_x, pivot_y, tile_cfg); a
+// Fortran READ of &READ_PARAMETERS skips it. Returns false on a malformed
+// group; absent group = zero-initialised options (reference behaviour).
+bool parse_b200_options(const std::string& text, ibfs_options_c& o, std::string& msg);
+
+// The namelist written when input/ibfs.inp is absent (parameters.f90:64-66).
+std::string format_read_parameters(const ibfs_params_c& p);
+
+struct Geometry {
+  std::vector<double> x, y;
+  std::vector<int> bodyno;
+};
+bool read_geometry(const std::string& path, Geometry& g, std::string& msg);
+// circle(ds, 1, 0, 0) -- the primitive the reference falls back to when
+// geom.inp is absent (grid.f90:353, 496-520).
+Geometry default_geometry(const ibfs_params_c& p);
+
+// Fortran unformatted sequential records (gfortran layout: 4-byte
+// little-endian length markers around the payload; payloads above
+// 2147483639 bytes are split into subrecords, the leading marker negative
+// when the record continues, the trailing marker negative when it continued
+// from the previous subrecord).
+bool write_record(const std::string& path, const std::vector<const double*>& parts,
+                  const std::vector<size_t>& counts, std::string& msg);
+bool read_record(const std::string& path, const std::vector<double*>& parts, const std::vector<size_t>& counts,
+                 std::string& msg);
+
+// One list-directed line "it v1 v2 ..." in the spacing gfortran uses for
+// default INTEGER and REAL(8) items (values written with 17 significant
+// digits, so they read back exactly).
+std::string list_directed(int it, const std::vector<double>& v);
+
+std::string file_text(const std::string& path, bool& ok);
+bool file_exists(const std::string& path);
+
+}  // namespace ibfs_host

@@ -8,6 +8,7 @@ Mirrors the reference's driver flow (src/main.f90:42-54): create (setup +
 setup_variables), optional restart/Cholesky load, then advance per step.
 """
 import ctypes
+import warnings
 import os
 
 import numpy as np
@@ -163,7 +164,10 @@ class Solver:
         except Exception:
             pass
 
-    def _check(self, rc):
+    def _check(self, rc, step=False):
+        if rc == 3 and step:  # IBFS_ERR_CG_MAXITER: the reference's warning; the step completed
+            warnings.warn("IBFS: " + lib().ibfs_last_error(self.h).decode(), RuntimeWarning, stacklevel=3)
+            return
         if rc != 0:
             raise IbfsError(rc, lib().ibfs_last_error(self.h).decode())
 
@@ -198,12 +202,12 @@ class Solver:
         circ, slip = np.zeros(s["nlev"]), np.zeros(1)
         bv = None if body_vel is None else np.ascontiguousarray(body_vel, dtype=np.float64)
         self._check(lib().ibfs_advance(self.h, ctypes.byref(self.itime), _p(bv), _p(fx), _p(fy),
-                                       _p(circ), _p(slip)))
+                                       _p(circ), _p(slip)), step=True)
         return dict(fx=fx, fy=fy, circ=circ, slip=float(slip[0]))
 
     def advance_n(self, nsteps, want_hist=True):
         hist = np.zeros(nsteps * self.stride) if want_hist else None
-        self._check(lib().ibfs_advance_n(self.h, nsteps, _p(hist)))
+        self._check(lib().ibfs_advance_n(self.h, nsteps, _p(hist)), step=True)
         self.itime.value += nsteps
         return hist.reshape(nsteps, self.stride) if want_hist else None
 
@@ -216,7 +220,7 @@ class Solver:
         bv = None if body_vel is None else np.ascontiguousarray(body_vel, dtype=np.float64)
         if bv is not None:
             assert bv.size == sum(s["nf"] for s in self.sizes), "body_vel must hold every case's Nf values"
-        self._check(lib().ibfs_batch_advance(self.h, _p(bv), _p(out)))
+        self._check(lib().ibfs_batch_advance(self.h, _p(bv), _p(out)), step=True)
         self.itime.value += 1
         return out
 

@@ -25,7 +25,9 @@ extern "C" {
 #define IBFS_OK 0
 #define IBFS_ERR_GRID 1        /* m or n not divisible by 4 (grid.f90:67-69)          */
 #define IBFS_ERR_CHOL 2        /* non-positive pivot, 'choldc failed' (operators.f90:784) */
-#define IBFS_ERR_CG_MAXITER 3  /* CG used cg_max_iter iterations (operators.f90:435-438) */
+#define IBFS_ERR_CG_MAXITER 3  /* CG used cg_max_iter iterations (operators.f90:435-438);
+                                  a warning, as in the reference: the step is complete and
+                                  its outputs are returned                               */
 #define IBFS_ERR_CUDA 4        /* CUDA runtime error; see ibfs_last_error              */
 #define IBFS_ERR_IO 5          /* restart / Cholesky file read or write failed         */
 #define IBFS_ERR_TIMEOUT 6     /* a bounded device wait gave up                        */
@@ -100,9 +102,11 @@ int ibfs_get_cholesky(const ibfs_handle* h, int icase, double* cholmat, double* 
 
 /* preprocess (operators.f90:29-59): A = [a_times(e_1) ... a_times(e_Nf)] built
  * as one multi-right-hand-side pass on the GPU, then choldc on the GPU. Runs
- * for every stationary case without a factor; ibfs_advance calls it at
- * itime == 1 as the reference does. Returns IBFS_ERR_CHOL on a non-positive
- * pivot. */
+ * for every stationary case without a factor; ibfs_advance, ibfs_advance_n
+ * and ibfs_batch_advance call it when a stationary case has none (the
+ * reference's preprocess at itime == 1 reads input/ibfs.chd instead when that
+ * file exists: give the factor with ibfs_set_cholesky before the first step).
+ * Returns IBFS_ERR_CHOL on a non-positive pivot. */
 int ibfs_precompute(ibfs_handle* h);
 
 /* advance (operators.f90:62-188) of a single-case handle. *itime is

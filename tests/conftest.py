@@ -6,6 +6,7 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "ibfs-if2d_b200")
 for sub in ("oracle", "ibfs-if2d_b200", os.path.join("tests", "golden")):
     p = os.path.join(ROOT, sub)
     if p not in sys.path:

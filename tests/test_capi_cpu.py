@@ -5,6 +5,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -40,3 +41,24 @@ def test_binding_matches_header(so_path):
 def test_kernels_are_sm100a(so_path):
     out = subprocess.run(["cuobjdump", "--list-elf", so_path], capture_output=True, text=True).stdout
     assert "sm_100a" in out
+
+
+def test_error_statuses_without_gpu(so_path):
+    """Argument and grid checks run before any CUDA call: the statuses and
+    messages of the reference's STOPs (grid.f90:67-69) come back on a host
+    without a GPU."""
+    import ibfs_capi as C
+    L = C.lib()
+    h = ctypes.c_void_p()
+    xb = np.zeros(4)
+    yb = np.linspace(-0.2, 0.2, 4)
+    p = C.make_params(30, 32, 0.01, 100.0, 3)  # m not divisible by 4
+    rc = L.ibfs_create(ctypes.byref(p), None, 4, C._p(xb), C._p(yb), None, ctypes.byref(h))
+    assert rc == 1 and h.value is None
+    assert b"divisible by 4" in L.ibfs_last_error(None)
+    rc = L.ibfs_create(None, None, 4, C._p(xb), C._p(yb), None, ctypes.byref(h))
+    assert rc == 7
+    rc = L.ibfs_case_sizes(None, 0, *([None] * 6))
+    assert rc == 7
+    assert L.ibfs_advance_n(None, 1, None) == 7
+    assert L.ibfs_batch_advance(None, None, None) == 7

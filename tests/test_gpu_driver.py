@@ -1,0 +1,93 @@
+"""The host driver (ibfs_gpu) run end to end in a reference-style run
+directory: its force.dat / restart records against the oracle, a restart from
+a .var record continuing the run exactly, and input/ibfs.chd reused."""
+import os
+import shutil
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+import workloads as W
+from conftest import PKG
+
+pytestmark = pytest.mark.gpu
+
+DRIVER = os.path.join(PKG, "ibfs_gpu")
+M, LEV, DT, RE, STEPS = 32, 3, 0.01, 100.0, 6
+
+
+def setup_dir(d, istart=0):
+    os.makedirs(d / "input", exist_ok=True)
+    (d / "input" / "ibfs.inp").write_text(
+        f" &READ_PARAMETERS ISTART = {istart}, ISTOP = {STEPS}, ISAVE = 3, M = {M},\n N = {M}, DT = {DT}, "
+        f"RE = {RE}, CGTOL = 1.E-7, CG_MAX_ITER = 3000,\n UNIF_FLOW = T, LEN = 4.0, OFFSETX = 2, OFFSETY = 2, "
+        f"MGRIDLEV = {LEV},\n MAKE_VORTEX = F, STATIONARY = T,\n /\n")
+    xb, yb = W.circle(4.0 / M)
+    lines = [f"{len(xb)}"] + [f" {float(x)!r} {float(y)!r} 0" for x, y in zip(xb, yb)]
+    (d / "input" / "geom.inp").write_text("\n".join(lines) + "\n")
+    return xb, yb
+
+
+def run(d):
+    r = subprocess.run([DRIVER, "-C", str(d)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout[-2000:]
+    return r
+
+
+def table(path):
+    return np.array([[float(v) for v in line.split()] for line in open(path) if line.strip()])
+
+
+def read_record(path):
+    raw = open(path, "rb").read()
+    n = struct.unpack("<i", raw[:4])[0]
+    assert struct.unpack("<i", raw[4 + n:8 + n])[0] == n
+    return np.frombuffer(raw[4:4 + n], dtype="<f8")
+
+
+@pytest.mark.skipif(not os.path.exists(DRIVER), reason="driver not built")
+def test_driver_run_restart_and_cholesky_file(tmp_path):
+    a = tmp_path / "a"
+    xb, yb = setup_dir(a)
+    run(a)
+    f = table(a / "output" / "force.dat")
+    assert f.shape == (STEPS, 3) and list(f[:, 0]) == list(range(1, STEPS + 1))
+    assert table(a / "output" / "circ.dat").shape == (STEPS, 1 + LEV)
+    assert table(a / "output" / "slip.dat").shape == (STEPS, 2)
+    assert (a / "input" / "ibfs.chd").exists()
+    # against the oracle, step by step
+    oc = O.Case(O.make_params(M, M, DT, RE, LEV), xb, yb)
+    ref = []
+    for _ in range(STEPS):
+        rc, o = oc.advance()
+        assert rc == 0
+        ref.append((o["fx"][0], o["fy"][0]))
+    ref = np.array(ref)
+    cd = np.abs(ref[:, 0]).max()
+    assert np.abs(f[:, 1:] - ref).max() / cd < 1e-10
+    rec = read_record(a / "output" / "ibfs0000006.var")
+    so = oc.get_state()
+    ns = (M - 1) ** 2
+    om = rec[:ns * LEV]
+    assert np.abs(om - so["omega"]).max() / np.abs(so["omega"]).max() < 1e-10
+    # restart from the step-3 record continues the run exactly
+    b = tmp_path / "b"
+    setup_dir(b, istart=3)
+    os.makedirs(b / "output")
+    shutil.copy(a / "output" / "ibfs0000003.var", b / "output")
+    shutil.copy(a / "input" / "ibfs.chd", b / "input")
+    run(b)
+    fb_ = open(b / "output" / "force.dat").read().splitlines()
+    fa_ = open(a / "output" / "force.dat").read().splitlines()
+    assert fb_ == fa_[3:]
+    assert np.array_equal(read_record(b / "output" / "ibfs0000006.var"), rec)
+    # a fresh run that finds input/ibfs.chd reads it instead of recomputing
+    c = tmp_path / "c"
+    setup_dir(c)
+    shutil.copy(a / "input" / "ibfs.chd", c / "input")
+    r = run(c)
+    assert "Reading Cholesky premade decomposition" in r.stdout
+    assert open(c / "output" / "force.dat").read() == open(a / "output" / "force.dat").read()

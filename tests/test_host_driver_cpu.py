@@ -1,0 +1,98 @@
+"""Host driver (ibfs-if2d_b200/ibfs_gpu) without a GPU: the reference's input
+files are read the way the Fortran program reads them (namelist
+&READ_PARAMETERS, parameters.f90:48-69; geom.inp, grid.f90:270-277; the
+unformatted restart record, variables.f90:141-175), checked through
+--dry-run, which stops before any CUDA call."""
+import json
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG
+
+DRIVER = os.path.join(PKG, "ibfs_gpu")
+
+pytestmark = pytest.mark.skipif(not os.path.exists(DRIVER), reason="driver not built (make -C ibfs-if2d_b200)")
+
+
+def run(d, *args):
+    r = subprocess.run([DRIVER, "-C", str(d), "--dry-run", *args], capture_output=True, text=True, timeout=60)
+    return r.returncode, r.stdout, r.stderr
+
+
+def write_inp(d, text):
+    os.makedirs(d / "input", exist_ok=True)
+    (d / "input" / "ibfs.inp").write_text(text)
+
+
+def fortran_record(path, arrays):
+    """gfortran sequential unformatted record: 4-byte length, payload, 4-byte length."""
+    payload = b"".join(np.ascontiguousarray(a, dtype="<f8").tobytes() for a in arrays)
+    with open(path, "wb") as f:
+        f.write(struct.pack("<i", len(payload)) + payload + struct.pack("<i", len(payload)))
+
+
+def test_namelist_reference_style(tmp_path):
+    # list-directed style of the reference's input file: upper case, commas,
+    # reals with a trailing '.' and an E exponent, logicals T/F
+    write_inp(tmp_path, " &READ_PARAMETERS ISTART = 0, ISTOP = 7, ISAVE = 3, M = 64,\n"
+                        " N = 48, DT = 0.0025, RE = 150., CGTOL = 1.E-9, CG_MAX_ITER = 500, \n"
+                        " UNIF_FLOW = T, LEN = 4.0, OFFSETX = 2, OFFSETY = 1.5D0, MGRIDLEV = 3, \n"
+                        " MAKE_VORTEX = F, STATIONARY = T,\n /\n")
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    p = json.loads(out)
+    assert (p["istart"], p["istop"], p["isave"], p["m"], p["n"]) == (0, 7, 3, 64, 48)
+    assert (p["dt"], p["re"], p["cgtol"], p["cg_max_iter"]) == (0.0025, 150.0, 1e-9, 500)
+    assert (p["unif_flow"], p["len"], p["offsetx"], p["offsety"]) == (1, 4.0, 2.0, 1.5)
+    assert (p["mgridlev"], p["make_vortex"], p["stationary"]) == (3, 0, 1)
+    assert p["precision"] == 0 and p["tile_cfg"] == -1
+    # no geom.inp: circle of diameter 1 at the origin, INT(pi/ds) points (grid.f90:353, 512)
+    assert p["nb"] == int(np.pi * 64 / 4.0) and abs(p["x0"] - 0.5) < 1e-15 and p["y0"] == 0.0
+
+
+def test_options_group_and_geometry(tmp_path):
+    write_inp(tmp_path, "&read_parameters m=32, n=32, len=4.0, offsetx=2.0, offsety=2.0, stationary=.true. /\n"
+                        "&B200_OPTIONS PRECISION=1, CG_RELATIVE=T, TILE_CFG=2 /\n")
+    (tmp_path / "input" / "geom.inp").write_text("3\n 0.1 0.2 0\n -0.25 0.5E-1 0\n 0.3 -0.1 0\n")
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    p = json.loads(out)
+    assert (p["precision"], p["cg_relative"], p["tile_cfg"]) == (1, 1, 2)
+    assert (p["nb"], p["x0"], p["y0"]) == (3, 0.1, 0.2)
+    # fields not in the file keep the reference defaults (parameters.f90:12-31)
+    assert (p["istop"], p["isave"], p["dt"], p["re"], p["mgridlev"]) == (400, 25, 0.005, 300.0, 4)
+
+
+def test_restart_record(tmp_path):
+    m = n = 32
+    L = 3
+    write_inp(tmp_path, f"&READ_PARAMETERS ISTART=12, ISTOP=14, M={m}, N={n}, MGRIDLEV={L}, LEN=4., "
+                        "OFFSETX=2., OFFSETY=2., STATIONARY=T /\n")
+    (tmp_path / "input" / "geom.inp").write_text("2\n 0.0 0.0 0\n 0.1 0.0 0\n")
+    os.makedirs(tmp_path / "output", exist_ok=True)
+    ns, nq = (m - 1) * (n - 1), (m + 1) * n + (n + 1) * m
+    rng = np.random.default_rng(3)
+    parts = [rng.standard_normal(ns * L), rng.standard_normal(4), rng.standard_normal(ns * L),
+             rng.standard_normal(nq * L), rng.standard_normal(nq * L)]
+    fortran_record(tmp_path / "output" / "ibfs0000012.var", parts)
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    sums = json.loads(out)["var_sums"]
+    assert np.allclose(sums, [a.sum() for a in parts], rtol=0, atol=1e-9)
+    # a record too short for the grid is refused
+    fortran_record(tmp_path / "output" / "ibfs0000012.var", parts[:3])
+    rc, out, err = run(tmp_path)
+    assert rc != 0 and "record holds" in err
+
+
+def test_bad_namelist(tmp_path):
+    write_inp(tmp_path, "&READ_PARAMETERS M=32, NOSUCH=3 /\n")
+    rc, out, err = run(tmp_path)
+    assert rc != 0 and "NOSUCH" in err
+    write_inp(tmp_path, "&READ_PARAMETERS M=3.5 /\n")
+    rc, out, err = run(tmp_path)
+    assert rc != 0 and "bad value" in err
