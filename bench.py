@@ -127,6 +127,24 @@ def dist_setup():
     return ws, rank, local
 
 
+def max_over_ranks(x, pg):
+    """Device time of the slowest rank (every rank calls this, in the same
+    order, so the collective sequence stays identical across ranks)."""
+    if pg is None:
+        return float(x)
+    import torch
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(cells_per_rank_step, steps, ws, tot_ms):
+    """Whole-job throughput: the cell-updates of all ranks over the slowest
+    rank's device time."""
+    return cells_per_rank_step * steps * ws / (tot_ms / 1e3)
+
+
 def peaks():
     try:
         p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -329,11 +347,8 @@ def run_ours(args):
         torch.cuda.nvtx.range_pop()
         tot_ms = g.last_ms()
         time.sleep(0.25)
-    if pg:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = cells * args.steps * ws / (tot_ms / 1e3)
+    tot_ms = max_over_ranks(tot_ms, pg)
+    value = aggregate(cells, args.steps, ws, tot_ms)
     ms_per_step = tot_ms / args.steps
     kern = g.kernels_per_step()
 
@@ -348,10 +363,7 @@ def run_ours(args):
     for _ in range(args.steps):
         g.batch_advance(bvel, out=row)
     te = time.perf_counter() - te
-    if pg:
-        t = torch.tensor([te], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        te = float(t.item())
+    te = max_over_ranks(te, pg)
     e2e = {"value": cells * args.steps * ws / te, "unit": UNIT, "h2d_bytes_per_step": 8 * sum_nf,
            "d2h_bytes_per_step": 8 * g.stride, "call": "ibfs_batch_advance", "ms_per_step": te / args.steps * 1e3}
 

@@ -77,6 +77,27 @@ def cells_per_step(cases, nlev):
     return int(sum(L * c["m"] * c["n"] for c, L in zip(cases, nlev)))
 
 
+def case_cost(c):
+    """Relative cost of one step of a case: (3L+1) sine-transform solves of
+    (m-1)^2 (m-1)-long contractions dominate, so ~ (3L+1) m^3."""
+    return (3 * c["levels"] + 1) * float(c["m"]) ** 3
+
+
+def shard(cases, rank, world):
+    """Indices of the cases one of `world` GPUs advances when a batch is split
+    across GPUs (independent cases: no exchange step between shards). Greedy
+    longest-first assignment to the least-loaded rank, deterministic, so that
+    every rank computes the same partition without communicating."""
+    order = sorted(range(len(cases)), key=lambda i: (-case_cost(cases[i]), i))
+    load = [0.0] * world
+    owner = [0] * len(cases)
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += case_cost(cases[i])
+    return [i for i in range(len(cases)) if owner[i] == rank]
+
+
 def solver_args(cases, capi, precision=0):
     """Params / bodies / options lists for ibfs_capi.Solver."""
     params = [capi.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"]) for c in cases]
