@@ -317,7 +317,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
     pk, src = peaks()
-    cases = W.batch(BATCH["ncases"], seed=SEED)
+    cases = W.batch(BATCH["ncases"], seed=SEED)[:args.ncases]
     params, bodies, opts = W.solver_args(cases, C, 1)
     t0 = time.perf_counter()
     g = C.Solver(params, bodies, opts)
@@ -430,7 +430,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3+f64",
             "data": "synthetic (seeded cases of the named shapes; no dataset)",
-            "config": dict(BATCH, cells_per_step=cells, form="batched split-precision",
+            "config": dict(BATCH, ncases=ncase, cells_per_step=cells, form="batched split-precision",
                            l2="inputs larger than L2 (~9 GB resident state), no flush",
                            parallelism="replicas" if ws > 1 else "single GPU",
                            create_s=t_create, precompute_s=t_pre),
@@ -526,6 +526,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="batch", choices=["batch", "plain", "precision"])
     ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--ncases", type=int, default=256,
+                    help="first N cases of the seeded batch (a smaller case for profiler captures)")
     ap.add_argument("--no-extras", action="store_true",
                     help="headline batch measurement only (no FP64 / plate / adjoint / CPU legs)")
     ap.add_argument("--ref-procs", type=int, default=128)
