@@ -1207,6 +1207,7 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
     IBFS_CUDA_CHECK(cudaMemcpy(s.vort, in, ns * sizeof(double), cudaMemcpyHostToDevice));
     if (h->precision == 1) {
       rc = precision_apply_op(h->prec, op, ds, s, st);
+      if (rc) rc = fail(rc, precision_error());
       dout = s.omega;
     } else {
       if (op == 0) {

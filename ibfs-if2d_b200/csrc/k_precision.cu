@@ -54,9 +54,19 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
-// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Every wait gives up after this long (a healthy wait lasts microseconds).
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+
+// Bounded wait for the phase with the given parity (try_wait may suspend the
+// thread between polls); false after kWaitLimitNs.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 20); ++it) {
+  uint64_t t0 = 0;
+  for (;;) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P;\n\t"
@@ -66,14 +76,17 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    const uint64_t t = global_ns();  // the clock is read only once a poll has failed
+    if (t0 == 0) t0 = t;
+    else if (t - t0 > kWaitLimitNs) return false;
   }
-  return false;
 }
 
 // Bounded spin without suspension, for the single producer / MMA threads whose
-// waits sit on the critical path of every K block; false on timeout.
+// waits sit on the critical path of every K block; false after kWaitLimitNs.
 __device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 26); ++it) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P;\n\t"
@@ -83,8 +96,24 @@ __device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 255) == 255) {  // no clock read on the fast path
+      const uint64_t t = global_ns();
+      if (t0 == 0) t0 = t;
+      else if (t - t0 > kWaitLimitNs) return false;
+    }
   }
-  return false;
+}
+
+// A wait that gave up: flag the error (bit 2 of status[0]) and, for the first
+// one, record where: status[1] = role (1 producer/stage free, 2 MMA/accumulator
+// free, 3 MMA/stage loaded, 4 epilogue/accumulator ready), status[2] = block,
+// status[3] = pipeline step.
+__device__ __forceinline__ void report_timeout(int* status, int role, int step) {
+  atomicOr(status, 2);
+  if (atomicCAS(status + 1, 0, role) == 0) {
+    status[2] = (int)blockIdx.x;
+    status[3] = step;
+  }
 }
 
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
@@ -533,7 +562,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       const int ns = d.nprod == 3 ? 2 : 3;  // slices per operand
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g & 1;
-        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g >> 1) + 1) & 1)) { to = true; break; }
+        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g >> 1) + 1) & 1)) { report_timeout(status, 1, g); to = true; break; }
         const uint32_t fb = full0 + 8 * s;
         mbar_expect_tx(fb, 2 * ns * AB);
         const uint32_t st = sbase + s * SB;
@@ -550,7 +579,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     int g = 0, t = 0;
     for (int w = blockIdx.x; w < nwork && !to; w += G, t++) {
       const int a = t & 1, u = t >> 1;
-      if (t >= 2 && !mbar_spin(acce0 + 8 * a, (u - 1) & 1)) { to = true; break; }
+      if (t >= 2 && !mbar_spin(acce0 + 8 * a, (u - 1) & 1)) { report_timeout(status, 2, t); to = true; break; }
       tc_fence_after();
       const TcDesc& d = descs[work[w].desc];
       const int nk = d.Kp / BK;
@@ -558,7 +587,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       const uint32_t acc = tmem + a * 128;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g & 1;
-        if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1)) { to = true; break; }
+        if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1)) { report_timeout(status, 3, g); to = true; break; }
         tc_fence_after();
         // stage base descriptor; operand tiles and K steps are immediate
         // offsets (16-byte units) on its address field
@@ -583,7 +612,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     int t = 0;
     for (int w = blockIdx.x; w < nwork; w += G, t++) {
       const int a = t & 1, u = t >> 1;
-      if (!mbar_wait(accf0 + 8 * a, u & 1)) { to = true; break; }
+      if (!mbar_wait(accf0 + 8 * a, u & 1)) { report_timeout(status, 4, t); to = true; break; }
       tc_fence_after();
       const TcDesc& d = descs[work[w].desc];
       const int tile = work[w].tile;
@@ -596,7 +625,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     }
   }
   __syncwarp();
-  if (__syncthreads_or(to) && tid == 0) atomicOr(status, 2);
+  __syncthreads_or(to);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, 256);
@@ -1132,9 +1161,13 @@ int precision_apply_op(PrecisionPlan* pp, int op, const DevCase* ds, const DevCa
   for (auto& e : P) e.fn();
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return 4;
-  int status = 0;
-  cudaMemcpy(&status, pp->status, sizeof(int), cudaMemcpyDeviceToHost);
-  return status ? 6 : 0;
+  int st4[4] = {0, 0, 0, 0};
+  cudaMemcpy(st4, pp->status, sizeof(st4), cudaMemcpyDeviceToHost);
+  if (!st4[0]) return 0;
+  cudaMemset(pp->status, 0, sizeof(st4));
+  g_perr = "tensor-core GEMM: a bounded wait gave up (role " + std::to_string(st4[1]) + ", block " +
+           std::to_string(st4[2]) + ", step " + std::to_string(st4[3]) + ")";
+  return 6;
 }
 
 }  // namespace ibfs
