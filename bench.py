@@ -27,8 +27,9 @@ Beside the headline (N=1 only): the plain FP64 advance on the 400x400x5 flat
 plate at 30 deg (Re 300, dt 0.002; L2 flushed between steps) and its ratio to
 the headline, the batched FP64 advance of the same 256 cases, the split-vs-FP64
 force and field errors, a sequential sample (cases one handle at a time), the
-split-precision plate, and the adjoint/forward cost on the rotating cylinder
-(Re 150, 256x256x4, 126 points).
+split-precision plate, the adjoint/forward cost on the rotating cylinder
+(Re 150, 256x256x4, 126 points), and 32 pitching plates advanced together
+(512x512x5, CG force solve every step).
 
 `--impl reference` times the CPU restatement of the reference (the oracle, a
 port: the Fortran+FFTW reference cannot be built here) on all host cores, one
@@ -272,6 +273,25 @@ def plain_and_split_plate(C, torch, steps, warmup, flush):
     return plain, split
 
 
+def pitching_batch(C, steps=3, warmup=2):
+    """Config-5 shape: 32 flat plates pitching about mid-chord with amplitudes
+    U[5, 30] deg, Re 500, 512x512 cells x 5 levels, dt 0.001, FP64 CG force
+    solve to a relative residual of 1e-12 every step, advanced together."""
+    cases = W.pitching_batch(32, seed=SEED)
+    params, bodies, opts = W.solver_args(cases, C)
+    g = C.Solver(params, bodies, opts)
+    g.advance_n(warmup, want_hist=False)
+    g.advance_n(steps, want_hist=False)
+    ms = g.last_ms() / steps
+    cells = W.cells_per_step(cases, [s["nlev"] for s in g.sizes])
+    out = {"value": cells / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+           "cg_iterations_last_step": g.last_cg_iterations(), "kernels_per_step_outside_cg": g.kernels_per_step(),
+           "workload": "32 pitching plates (amplitude U[5,30] deg, f 0.25, mid-chord pivot), Re 500, "
+                       "512x512 cells x 5 levels, dt 0.001, FP64 CG to relative residual 1e-12"}
+    g.close()
+    return out
+
+
 def adjoint_cost(C, steps=100, K=50):
     """Rotating cylinder (Re 150, 256x256x4, 126 points, dt .004): the discrete
     adjoint of the mean lift over the last third of the horizon w.r.t. the
@@ -423,6 +443,7 @@ def run_ours(args):
             extras["ratio_vs_plain_fp64"] = value / plain["value"]
             extras["plate400_split"] = split
             extras["adjoint"] = adjoint_cost(C)
+            extras["pitching_batch"] = pitching_batch(C)
             cpu = cpu_sample_from_gpu(g, cases, sorted(int(x) for x in np.random.default_rng(SEED + 2).choice(
                 ncase, 6, replace=False)), args.cpu_steps)
         out = {
@@ -525,7 +546,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="batch", choices=["batch", "plain", "precision"])
-    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--ncases", type=int, default=256,
                     help="first N cases of the seeded batch (a smaller case for profiler captures)")
     ap.add_argument("--no-extras", action="store_true",

@@ -98,9 +98,33 @@ def shard(cases, rank, world):
     return [i for i in range(len(cases)) if owner[i] == rank]
 
 
+def pitching(m=512, levels=5, re=500.0, dt=0.001, amp_deg=20.0, freq=0.25, cgtol=1e-12):
+    """Flat plate of chord 1 pitching sinusoidally about mid-chord,
+    alpha(t) = amp sin(2 pi freq t), body points at spacing dx along the chord;
+    the force system is solved by CG to a relative residual of cgtol every step."""
+    c = case(m, levels, re, dt, "plate", aoa=0.0)
+    c.update(pitch_amp_deg=float(amp_deg), pitch_freq=float(freq), cgtol=float(cgtol))
+    return c
+
+
+def pitching_batch(ncases=32, seed=20261203, **kw):
+    """Pitching plates whose amplitudes are drawn uniformly from [5, 30] degrees."""
+    rng = np.random.default_rng(seed)
+    return [pitching(amp_deg=float(a), **kw) for a in rng.uniform(5.0, 30.0, ncases)]
+
+
 def solver_args(cases, capi, precision=0):
-    """Params / bodies / options lists for ibfs_capi.Solver."""
-    params = [capi.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"]) for c in cases]
+    """Params / bodies / options lists for ibfs_capi.Solver (pitching cases:
+    moving body, CG with a relative stop, motion on the device)."""
+    params, opts = [], []
+    for c in cases:
+        if "pitch_amp_deg" in c:
+            params.append(capi.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"], stationary=False,
+                                           cgtol=c["cgtol"]))
+            opts.append(capi.make_options(precision=precision, cg_relative=1, motion_kind=1,
+                                          pitch_amp_deg=c["pitch_amp_deg"], pitch_freq=c["pitch_freq"]))
+        else:
+            params.append(capi.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"]))
+            opts.append(capi.make_options(precision=precision))
     bodies = [(c["xb"], c["yb"]) for c in cases]
-    opts = [capi.make_options(precision=precision) for _ in cases]
     return params, bodies, opts

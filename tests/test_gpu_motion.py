@@ -69,3 +69,35 @@ def test_pitching_plate(precision):
     tol = 1e-9 if precision == 0 else 1e-7
     assert np.abs(fg - fo).max() / np.abs(fo).max() < tol
     assert rel(g.get_state()["omega"], oc.get_state()["omega"]) < tol
+
+
+def test_pitching_batch_equals_single_handles():
+    """Several pitching amplitudes advanced together (one launch per kernel,
+    CG iterations until every case has converged, converged cases idle) give
+    each case's single-handle result, and the first case follows the oracle."""
+    import workloads as W
+    cases = [W.pitching(m=48, levels=3, re=500.0, dt=0.01, amp_deg=a) for a in (5.0, 17.0, 30.0)]
+    params, bodies, opts = W.solver_args(cases, C)
+    g = C.Solver(params, bodies, opts)
+    hist = g.advance_n(5)
+    for ic in range(len(cases)):
+        s = C.Solver(params[ic], bodies[ic], opts[ic])
+        hs = s.advance_n(5)
+        assert rel(g.get_state(ic)["omega"], s.get_state()["omega"]) < 1e-13, ic
+        fb = np.array([g.outputs_of(hist[k], ic)["fx"][0] for k in range(5)])
+        fs = np.array([s.outputs_of(hs[k], 0)["fx"][0] for k in range(5)])
+        assert rel(fb, fs) < 1e-13, ic
+        s.close()
+    c = cases[0]
+    oc = O.Case(O.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"], stationary=False, cgtol=1e-12),
+                c["xb"], c["yb"], np.ones(len(c["xb"])))
+    oc.set_cg_relative(True)
+    fo = []
+    for k in range(1, 6):
+        x, y, v = pitch_state(c["xb"], c["yb"], k * c["dt"], c["pitch_amp_deg"], c["pitch_freq"])
+        oc.set_body(x, y)
+        rc, o = oc.advance(body_vel=v)
+        assert rc == 0
+        fo.append(o["fx"][0])
+    fb = np.array([g.outputs_of(hist[k], 0)["fx"][0] for k in range(5)])
+    assert rel(fb, fo) < 1e-9
