@@ -979,6 +979,21 @@ int ibfs_get_state(const ibfs_handle* h, int icase, double* omega, double* fb, d
   return IBFS_OK;
 }
 
+int ibfs_vertex_fields(ibfs_handle* h, int icase, int level, double* out) {
+  if (!h || icase < 0 || icase >= (int)h->cases.size() || !out) return fail(IBFS_ERR_ARG, "null argument or case");
+  const HostCase& c = h->cases[icase];
+  if (level < 1 || level > c.L) return fail(IBFS_ERR_ARG, "level outside 1..mgridlev");
+  if (!h->d_vertex) {
+    h->d_vertex = dalloc<double>(h, (size_t)5 * h->max_ns, false);
+    if (!h->d_vertex) return fail(IBFS_ERR_NOMEM, "vertex buffer");
+  }
+  launch_vertex(h->d_cases, icase, level, c.ns, h->d_vertex, h->st);
+  IBFS_CUDA_CHECK(cudaGetLastError());
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(out, h->d_vertex, sizeof(double) * 5 * (size_t)c.ns, cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  return IBFS_OK;
+}
+
 int ibfs_set_cholesky(ibfs_handle* h, int icase, const double* cholmat, const double* cholvec) {
   if (!h || icase < 0 || icase >= (int)h->cases.size() || !cholmat || !cholvec) return IBFS_ERR_ARG;
   HostCase& c = h->cases[icase];

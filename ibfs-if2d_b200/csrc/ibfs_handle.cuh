@@ -76,6 +76,7 @@ struct ibfs_handle {
   double* d_bvel = nullptr;   // every case's body velocities, contiguous in case order
   double* h_bvel = nullptr;   // pinned staging of the same
   int sum_nf = 0;
+  double* d_vertex = nullptr;  // 5 x max_ns, vertex fields of the Tecplot export (allocated on first use)
   AdjPlan* adj = nullptr;
 };
 

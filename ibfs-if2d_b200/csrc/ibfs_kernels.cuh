@@ -60,6 +60,7 @@ std::vector<int2> block_map(const std::vector<int>& counts);
 __host__ __device__ inline int coarsify_count(int m, int n) {
   return (3 * m / 4 - (m / 4 + 2) + 1) * (3 * n / 4 - (n / 4 + 2) + 1);
 }
+void launch_vertex(const DevCase* cases, int c, int k, int ns, double* out, cudaStream_t st);
 void launch_rhs(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, int first,
                 cudaStream_t st);
 void launch_coarsify(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, cudaStream_t st);

@@ -219,6 +219,37 @@ __global__ void __launch_bounds__(256) k_regrot(const DevCase* __restrict__ case
   for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) regrot_at(C, t);
 }
 
+// Vertex fields of level k for the Tecplot export (write_tecplot,
+// operators.f90:723-737), with del = 2^(k-1) delta and etf = reg(fb) on the
+// level-1 faces (the reference uses it for every level), each in the
+// reference's evaluation order:
+//   u = 0.5 (q(u(i,j)) + q(u(i,j-1)) + q0(u(i,j)) + q0(u(i,j-1))) / del
+//   v = 0.5 (q(v(i,j)) + q(v(i-1,j)) + q0(v(i,j)) + q0(v(i-1,j))) / del
+//   etfx = delta (etf(u(i,j)) + etf(u(i,j-1))) / dt, etfy likewise on v
+//   vort = omega(i,j,k) / del / del
+// out: [5][(m-1)(n-1)], node (i,j) with i = 2..m fastest.
+__global__ void k_vertex(const DevCase* __restrict__ cases, int c, int k, double* __restrict__ out) {
+  const DevCase& C = cases[c];
+  const int m = C.m, n = C.n;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= C.ns) return;
+  const int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
+  const double fac = (double)(1 << (k - 1));
+  const double del = fac * C.delta;
+  const double* q = C.q + (size_t)(k - 1) * C.nq;
+  const double* q0 = C.q0 + (size_t)(k - 1) * C.nq;
+  const int u1 = uoff(i, j, m), u0 = uoff(i, j - 1, m), v1 = voff(i, j, m, n), v0 = voff(i - 1, j, m, n);
+  out[t] = 0.5 * (q[u1] + q[u0] + q0[u1] + q0[u0]) / del;
+  out[C.ns + t] = 0.5 * (q[v1] + q[v0] + q0[v1] + q0[v0]) / del;
+  out[2 * (size_t)C.ns + t] = C.delta * (reg_face(C, C.fb, u1) + reg_face(C, C.fb, u0)) / C.dt;
+  out[3 * (size_t)C.ns + t] = C.delta * (reg_face(C, C.fb, v1) + reg_face(C, C.fb, v0)) / C.dt;
+  out[4 * (size_t)C.ns + t] = C.omega[(size_t)(k - 1) * C.ns + t] / del / del;
+}
+
+void launch_vertex(const DevCase* cases, int c, int k, int ns, double* out, cudaStream_t st) {
+  k_vertex<<<(ns + 255) / 256, 256, 0, st>>>(cases, c, k, out);
+}
+
 // regT (operators.f90:531-546) of one face field, gathered per force in the
 // reference's scatter order (ascending face index).
 __device__ __forceinline__ double regT_force(const DevCase& C, const double* __restrict__ h, int f) {

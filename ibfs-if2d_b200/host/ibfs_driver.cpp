@@ -18,9 +18,13 @@
 //              (operators.f90:176-188, 549-699)
 // Actuator points (bodyno < 0, grid.f90:579-718) are not supported.
 //
-//   ibfs_gpu [-C dir] [--dry-run]
+//   ibfs_gpu [-C dir] [--dry-run | --post]
 // --dry-run reads and checks the inputs (and a restart record when
 // istart > 0) and prints them as JSON without touching the GPU.
+// --post is the reference's post-processing program (post.f90): for every
+// step istart..istop that has a restart record (it % isave == 0 or istop; the
+// initial state for it = 0) it writes post/ibfs_g<level>t<it>_vel.dat for each
+// level, the Tecplot files of write_tecplot (operators.f90:702-763).
 #include <sys/stat.h>
 #include <unistd.h>
 
@@ -71,13 +75,14 @@ std::string var_name(int it) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  bool dry = false;
+  bool dry = false, post = false;
   for (int a = 1; a < argc; a++) {
     if (!std::strcmp(argv[a], "--dry-run")) dry = true;
+    else if (!std::strcmp(argv[a], "--post")) post = true;
     else if (!std::strcmp(argv[a], "-C") && a + 1 < argc) {
       if (::chdir(argv[++a]) != 0) return stop(std::string("cannot enter ") + argv[a], 2);
     } else {
-      std::fprintf(stderr, "usage: ibfs_gpu [-C dir] [--dry-run]\n");
+      std::fprintf(stderr, "usage: ibfs_gpu [-C dir] [--dry-run | --post]\n");
       return 2;
     }
   }
@@ -180,6 +185,33 @@ int main(int argc, char** argv) {
     std::printf("Reading Cholesky premade decomposition...\n");
     return ibfs_set_cholesky(h, 0, cholmat.data(), cholvec.data()) == IBFS_OK;
   };
+  if (post) {  // post.f90: Tecplot files of every saved step
+    ::mkdir("post", 0755);
+    std::vector<double> fields((size_t)5 * ns);
+    for (int it = p.istart; it <= p.istop; it++) {
+      if (!(it % p.isave == 0 || it == p.istop)) continue;
+      if (it > 0) {
+        if (!read_record(var_name(it), {omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data()},
+                         {omega.size(), fb.size(), rhs_old.size(), q.size(), q0.size()}, msg))
+          return stop(msg, 5);
+        rc = ibfs_set_state(h, 0, omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data());
+        if (rc) return stop(std::string("ibfs_set_state: ") + ibfs_last_error(h), 10 + rc);
+      }
+      std::printf(" Post-processing: itime = %12d\n", it);
+      for (int k = 1; k <= L; k++) {
+        rc = ibfs_vertex_fields(h, 0, k, fields.data());
+        if (rc) return stop(std::string("ibfs_vertex_fields: ") + ibfs_last_error(h), 10 + rc);
+        char name[96];
+        std::snprintf(name, sizeof name, "post/ibfs_g%1dt%07d_vel.dat", k, it);
+        if (!write_tecplot(name, it, m, n, (double)(float)(1 << (k - 1)), p.len / (double)p.m, p.len,
+                           p.offsetx, p.offsety, fields.data(), msg))
+          return stop(msg, 5);
+      }
+    }
+    ibfs_destroy(h);
+    if (g_inf) std::fclose(g_inf);
+    return 0;
+  }
   if (p.istart > 0) {
     if (!read_record(var_name(p.istart), {omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data()},
                      {omega.size(), fb.size(), rhs_old.size(), q.size(), q0.size()}, msg))

@@ -373,6 +373,55 @@ std::string list_directed(int it, const std::vector<double>& v) {
   return s;
 }
 
+std::string fortran_E(double x, int w, int d) {
+  std::string body;
+  if (x == 0.0 || !std::isfinite(x)) {
+    if (!std::isfinite(x)) body = std::string(w, '*');
+    else body = "0." + std::string(d, '0') + "E+00";
+  } else {
+    char v[64];
+    std::snprintf(v, sizeof v, "%.*E", d - 1, std::fabs(x));  // D.DDDDE+XX, rounded to d digits
+    std::string t = v;
+    size_t e = t.find('E');
+    std::string digits = t.substr(0, 1) + t.substr(2, e - 2);
+    int ex = std::atoi(t.c_str() + e + 1) + 1;  // 0.DDDDD x 10^ex
+    char eb[16];
+    if (std::abs(ex) <= 99) std::snprintf(eb, sizeof eb, "E%c%02d", ex < 0 ? '-' : '+', std::abs(ex));
+    else std::snprintf(eb, sizeof eb, "%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
+    body = std::string(x < 0 ? "-" : "") + "0." + digits + eb;
+  }
+  if ((int)body.size() > w) return std::string(w, '*');
+  return std::string(w - body.size(), ' ') + body;
+}
+
+bool write_tecplot(const std::string& path, int it, int m, int n, double fac, double delta, double len,
+                   double offsetx, double offsety, const double* f, std::string& msg) {
+  FILE* o = std::fopen(path.c_str(), "w");
+  if (!o) {
+    msg = "cannot write " + path;
+    return false;
+  }
+  const double offx = (fac - 1.0) / 2.0 * len;
+  const double offy = (fac - 1.0) / 2.0 * delta * (double)(float)n;
+  const size_t ns = (size_t)(m - 1) * (n - 1);
+  std::fprintf(o, " TITLE     = \"IBFS V1.0 AT ITIME=%12d\"\n", it);
+  std::fprintf(o, " VARIABLES = \"x\"\n \"y\"\n \"u\"\n \"v\"\n \"etfx\"\n \"etfy\"\n \"vort\"\n");
+  std::fprintf(o, " ZONE T=\"Rectangular zone\"\n");
+  std::fprintf(o, " I=%12d, J=%12d, K=1, ZONETYPE=Ordered\n", m - 1, n - 1);
+  std::fprintf(o, " DATAPACKING=POINT\n DT=(SINGLE SINGLE SINGLE SINGLE SINGLE SINGLE SINGLE)\n");
+  for (int j = 2; j <= n; j++)
+    for (int i = 2; i <= m; i++) {
+      const size_t t = (size_t)(i - 2) + (size_t)(j - 2) * (m - 1);
+      std::string line = fortran_E(fac * delta * (double)(float)(i - 1) - offx - offsetx, 14, 5) +
+                         fortran_E(fac * delta * (double)(float)(j - 1) - offy - offsety, 14, 5);
+      for (int k = 0; k < 5; k++) line += fortran_E(f[k * ns + t], 14, 5);
+      std::fprintf(o, "%s\n", line.c_str());
+    }
+  bool ok = std::fclose(o) == 0;
+  if (!ok) msg = "write failed: " + path;
+  return ok;
+}
+
 std::string file_text(const std::string& path, bool& ok) {
   std::ifstream f(path);
   ok = (bool)f;

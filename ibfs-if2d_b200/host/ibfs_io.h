@@ -60,6 +60,17 @@ bool read_record(const std::string& path, const std::vector<double*>& parts, con
 // digits, so they read back exactly).
 std::string list_directed(int it, const std::vector<double>& v);
 
+// Fortran Ew.d editing of one value: 0.ddddd mantissa, two-digit exponent
+// with its sign (E+ee), or a three-digit exponent without the E.
+std::string fortran_E(double x, int w, int d);
+
+// One level's Tecplot file of write_tecplot (operators.f90:702-763): the
+// header, then per node (j outer, i inner) x, y and the five fields of
+// ibfs_vertex_fields in (8E14.5). fac = 2^(level-1); the offsets follow the
+// reference (offx = (fac-1)/2 len, offy = (fac-1)/2 delta n).
+bool write_tecplot(const std::string& path, int it, int m, int n, double fac, double delta, double len,
+                   double offsetx, double offsety, const double* fields, std::string& msg);
+
 std::string file_text(const std::string& path, bool& ok);
 bool file_exists(const std::string& path);
 

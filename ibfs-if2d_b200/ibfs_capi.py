@@ -25,7 +25,7 @@ EXPORTS = [
     "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
     "ibfs_advance", "ibfs_advance_n", "ibfs_batch_advance", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
-    "ibfs_last_cg_iterations", "ibfs_adjoint_run",
+    "ibfs_last_cg_iterations", "ibfs_adjoint_run", "ibfs_vertex_fields",
     "ibfs_last_error",
 ]
 
@@ -84,6 +84,7 @@ def lib():
         L.ibfs_advance.argtypes = [vp, _IP, _DP, _DP, _DP, _DP, _DP]
         L.ibfs_advance_n.argtypes = [vp, ctypes.c_int, _DP]
         L.ibfs_batch_advance.argtypes = [vp, _DP, _DP]
+        L.ibfs_vertex_fields.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP]
         L.ibfs_output_offset.argtypes = [vp, ctypes.c_int]
         L.ibfs_output_stride.argtypes = [vp]
         L.ibfs_apply_op.argtypes = [vp, ctypes.c_int, _DP, _DP]
@@ -223,6 +224,15 @@ class Solver:
         self._check(lib().ibfs_batch_advance(self.h, _p(bv), _p(out)), step=True)
         self.itime.value += 1
         return out
+
+    def vertex_fields(self, level, icase=0):
+        """write_tecplot's vertex fields of one level (1-based): dict of u, v,
+        etfx, etfy, vort, each (m-1)*(n-1) with i fastest."""
+        s = self.sizes[icase]
+        out = np.zeros(5 * s["ns"])
+        self._check(lib().ibfs_vertex_fields(self.h, icase, level, _p(out)))
+        f = out.reshape(5, s["ns"])
+        return dict(u=f[0], v=f[1], etfx=f[2], etfy=f[3], vort=f[4])
 
     def outputs_of(self, hist_row, icase=0):
         s = self.sizes[icase]

@@ -95,6 +95,13 @@ int ibfs_set_state(ibfs_handle* h, int icase, const double* omega, const double*
 int ibfs_get_state(const ibfs_handle* h, int icase, double* omega, double* fb, double* rhs_old,
                    double* q, double* q0);
 
+/* Vertex fields of one level for the Tecplot export (write_tecplot,
+ * operators.f90:702-763, the post-processing step after the advance):
+ * out[5][(m-1)*(n-1)], node (i,j) with i = 2..m fastest, the fields u, v,
+ * etfx, etfy, vort in the reference's order and arithmetic (etf = reg(fb) on
+ * the level-1 faces, del = 2^(level-1) delta). level is 1-based. */
+int ibfs_vertex_fields(ibfs_handle* h, int icase, int level, double* out);
+
 /* read_cholesky / write_cholesky payload (variables.f90:110-137): cholmat
  * (upper triangle = A, strict lower = factor) and cholvec (diagonal). */
 int ibfs_set_cholesky(ibfs_handle* h, int icase, const double* cholmat, const double* cholvec);

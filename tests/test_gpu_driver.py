@@ -91,3 +91,25 @@ def test_driver_run_restart_and_cholesky_file(tmp_path):
     r = run(c)
     assert "Reading Cholesky premade decomposition" in r.stdout
     assert open(c / "output" / "force.dat").read() == open(a / "output" / "force.dat").read()
+    # post-processing (post.f90): Tecplot files of the saved steps, every level
+    r = subprocess.run([DRIVER, "-C", str(a), "--post"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    from test_gpu_parity import vertex_reference
+    for it in (0, 3, 6):
+        for k in range(1, LEV + 1):
+            path = a / "post" / f"ibfs_g{k}t{it:07d}_vel.dat"
+            lines = open(path).read().splitlines()
+            assert lines[0].split("=")[-1].strip(' "') == str(it) and len(lines) == 12 + (M - 1) ** 2
+            data = np.array([[float(line[14 * c:14 * c + 14]) for c in range(7)] for line in lines[12:]])
+            fac, de = 2.0 ** (k - 1), 4.0 / M
+            ii, jj = np.meshgrid(np.arange(2, M + 1), np.arange(2, M + 1))
+            x = fac * de * (ii.ravel() - 1) - (fac - 1) / 2 * 4.0 - 2.0
+            y = fac * de * (jj.ravel() - 1) - (fac - 1) / 2 * de * M - 2.0
+            assert np.allclose(data[:, 0], x, rtol=1e-5, atol=1e-5) and np.allclose(data[:, 1], y, rtol=1e-5, atol=1e-5)
+            if it == 6:
+                ref = vertex_reference(oc, so, k, de, DT)
+                for c, f in enumerate(("u", "v", "etfx", "etfy", "vort")):
+                    # E14.5 keeps five significant digits: half a unit of the fifth,
+                    # plus the FP64 parity bar (1e-10 of the field) for values at roundoff level
+                    bar = 5.01e-5 * np.abs(ref[f]) + 1e-10 * np.abs(ref[f]).max() + 1e-300
+                    assert np.all(np.abs(data[:, 2 + c] - ref[f]) <= bar), (k, f)

@@ -86,3 +86,39 @@ def test_advance_n_graph_matches_single_steps():
     assert rel(b["omega"], a["omega"]) < 1e-13
     o = g2.outputs_of(hist[-1])
     assert np.isfinite(o["fx"]).all()
+
+
+def vertex_reference(oc, st, k, delta, dt):
+    """write_tecplot's vertex fields (operators.f90:723-737) restated in numpy
+    from a state and the oracle's reg, same evaluation order."""
+    m, n, nq = oc.m, oc.n, oc.nq
+    ns = (m - 1) * (n - 1)
+    om = st["omega"][(k - 1) * ns:k * ns]
+    q, q0 = st["q"][(k - 1) * nq:k * nq], st["q0"][(k - 1) * nq:k * nq]
+    etf = oc.reg(np.ascontiguousarray(st["fb"]))
+    de = 2.0 ** (k - 1) * delta
+    i, j = np.meshgrid(np.arange(2, m + 1), np.arange(2, n + 1))  # j outer, i inner = node order
+    i, j = i.ravel(), j.ravel()
+    u1, u0 = (i - 1) + (j - 1) * (m + 1), (i - 1) + (j - 2) * (m + 1)
+    v1, v0 = (m + 1) * n + (i - 1) + (j - 1) * m, (m + 1) * n + (i - 2) + (j - 1) * m
+    return dict(u=0.5 * (q[u1] + q[u0] + q0[u1] + q0[u0]) / de, v=0.5 * (q[v1] + q[v0] + q0[v1] + q0[v0]) / de,
+                etfx=delta * (etf[u1] + etf[u0]) / dt, etfy=delta * (etf[v1] + etf[v0]) / dt, vort=om / de / de)
+
+
+def test_vertex_fields_match_reference_export():
+    """ibfs_vertex_fields (the Tecplot export's arithmetic) on every level after
+    a few steps, against the numpy restatement on the oracle's state."""
+    m, lev, dt = 48, 3, 0.01
+    xb, yb = O.circle(4.0 / m, 1.0, 0.0, 0.0)
+    oc = O.Case(O.make_params(m, m, dt, 100.0, lev), xb, yb)
+    g = C.Solver(C.make_params(m, m, dt, 100.0, lev), (xb, yb))
+    for _ in range(4):
+        oc.advance()
+    g.advance_n(4, want_hist=False)
+    st = oc.get_state()
+    for k in range(1, lev + 1):
+        ref = vertex_reference(oc, st, k, 4.0 / m, dt)
+        got = g.vertex_fields(k)
+        for f in ("u", "v", "etfx", "etfy", "vort"):
+            scale = max(np.abs(ref[f]).max(), 1e-300)
+            assert np.abs(got[f] - ref[f]).max() / scale < 1e-10, (k, f)
