@@ -4,9 +4,11 @@
 // GPU: same run directory, same input files, same output files.
 //   input      input/ibfs.inp (&READ_PARAMETERS; written with the defaults if
 //              absent, parameters.f90:54-69), optional &B200_OPTIONS group
-//   setup      input/geom.inp, or a circle of diameter 1 at the origin when it
-//              is absent (grid.f90:252-353); grid checks and regularisation
-//              happen in ibfs_create
+//   setup      input/geom.inp; else input/geom.spec (the reference's primitives,
+//              one per line, written out as geom.inp); else a circle of diameter
+//              1 at the origin (grid.f90:252-353); the point spacing is checked
+//              against the grid; grid checks and regularisation happen in
+//              ibfs_create
 //   variables  istart = 0: zero (or uniform) flow; otherwise
 //              output/ibfsNNNNNNN.var and, for a stationary body,
 //              input/ibfs.chd (variables.f90:28-77)
@@ -131,8 +133,18 @@ int main(int argc, char** argv) {
     if (!read_geometry("input/geom.inp", geo, msg)) return stop(msg, 2);
     logline("Reading geometry from geom.inp");
     if (!dry) std::printf("Reading geometry from geom.inp\n");
+  } else if (file_exists("input/geom.spec")) {  // primitives -> geom.inp
+    bool ok = false;
+    std::string spec = file_text("input/geom.spec", ok);
+    if (!ok || !geometry_from_spec(spec, p.len / (double)p.m, geo, msg)) return stop("input/geom.spec: " + msg, 2);
+    if (!dry && !write_geometry("input/geom.inp", geo, msg)) return stop(msg, 2);
+    logline("Generated geometry from primitives (input/geom.spec) into geom.inp");
   } else {
     geo = default_geometry(p);
+  }
+  for (const std::string& w : spacing_warnings(geo, p.len / (double)p.m)) {
+    std::fprintf(stderr, "%s\n", w.c_str());
+    logline(w);
   }
   for (int b : geo.bodyno)
     if (b < 0) return stop("actuator points (bodyno < 0) are not supported by this driver", 2);
@@ -159,10 +171,13 @@ int main(int argc, char** argv) {
                 "\"re\": %.17g, \"cgtol\": %.17g, \"cg_max_iter\": %d, \"unif_flow\": %d, \"len\": %.17g, "
                 "\"offsetx\": %.17g, \"offsety\": %.17g, \"mgridlev\": %d, \"make_vortex\": %d, "
                 "\"stationary\": %d, \"precision\": %d, \"cg_relative\": %d, \"motion_kind\": %d, "
-                "\"tile_cfg\": %d, \"nb\": %d, \"x0\": %.17g, \"y0\": %.17g, \"var_sums\": [",
+                "\"tile_cfg\": %d, \"nb\": %d, \"x0\": %.17g, \"y0\": %.17g, \"xsum\": %.17g, \"ysum\": %.17g, "
+                "\"var_sums\": [",
                 p.istart, p.istop, p.isave, p.m, p.n, p.dt, p.re, p.cgtol, p.cg_max_iter, p.unif_flow, p.len,
                 p.offsetx, p.offsety, p.mgridlev, p.make_vortex, p.stationary, opt.precision, opt.cg_relative,
-                opt.motion_kind, opt.tile_cfg, nb, nb ? geo.x[0] : 0.0, nb ? geo.y[0] : 0.0);
+                opt.motion_kind, opt.tile_cfg, nb, nb ? geo.x[0] : 0.0, nb ? geo.y[0] : 0.0,
+                [&] { double t = 0.0; for (double v : geo.x) t += v; return t; }(),
+                [&] { double t = 0.0; for (double v : geo.y) t += v; return t; }());
     for (size_t i = 0; i < var_sums.size(); i++) std::printf("%s%.17g", i ? ", " : "", var_sums[i]);
     std::printf("]}\n");
     return 0;

@@ -3,6 +3,7 @@
 
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -252,6 +253,119 @@ Geometry default_geometry(const ibfs_params_c& p) {
     g.bodyno.push_back(0);
   }
   return g;
+}
+
+bool geometry_from_spec(const std::string& text, double ds, Geometry& g, std::string& msg) {
+  const double pi = 3.1415926535897932384;
+  std::istringstream in(text);
+  std::string line;
+  int ln = 0;
+  while (std::getline(in, line)) {
+    ln++;
+    size_t h = line.find('#');
+    if (h != std::string::npos) line = line.substr(0, h);
+    std::istringstream w(line);
+    std::string kind;
+    if (!(w >> kind)) continue;
+    kind = upper(kind);
+    auto bad = [&]() {
+      msg = "geometry spec line " + std::to_string(ln) + ": cannot read '" + line + "'";
+      return false;
+    };
+    auto add = [&](double x, double y, int b) {
+      g.x.push_back(x);
+      g.y.push_back(y);
+      g.bodyno.push_back(b);
+    };
+    if (kind == "VERTEX") {
+      double x, y;
+      int b;
+      if (!(w >> x >> y >> b)) return bad();
+      add(x, y, b);
+    } else if (kind == "LINE") {  // grid.f90:431-462
+      double len, aoa;
+      int b;
+      if (!(w >> len >> aoa >> b)) return bad();
+      const double angle = -aoa * pi / 180.0;
+      const double xle = -0.5 * len * std::cos(angle), yle = -0.5 * len * std::sin(angle);
+      const int npt = (int)(len / ds);
+      for (int i = 1; i <= npt + 1; i++) {
+        const double seg = (double)(float)(i - 1) * len / (double)(float)npt;
+        add(xle + seg * std::cos(angle), yle + seg * std::sin(angle), b);
+      }
+    } else if (kind == "SEGMENT") {  // grid.f90:465-493
+      double x1, y1, x2, y2;
+      int b;
+      if (!(w >> x1 >> y1 >> x2 >> y2 >> b)) return bad();
+      const double len = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+      const double angle = std::atan2(y2 - y1, x2 - x1);
+      const int npt = (int)(len / ds);
+      for (int i = 1; i <= npt - 1; i++) {
+        const double seg = (double)(float)i * len / (double)(float)npt;
+        add(x1 + seg * std::cos(angle), y1 + seg * std::sin(angle), b);
+      }
+    } else if (kind == "CIRCLE") {  // grid.f90:496-520
+      double dia, x, y;
+      int b;
+      if (!(w >> dia >> x >> y >> b)) return bad();
+      const int npt = (int)(pi * dia / ds);
+      for (int i = 1; i <= npt; i++) {
+        const double a = 2.0 * pi * (double)(float)(i - 1) / (double)(float)npt;
+        add(x + 0.5 * dia * std::cos(a), y + 0.5 * dia * std::sin(a), b);
+      }
+    } else {
+      msg = "geometry spec line " + std::to_string(ln) + ": unknown primitive '" + kind + "'";
+      return false;
+    }
+  }
+  if (g.x.empty()) {
+    msg = "geometry spec holds no points";
+    return false;
+  }
+  return true;
+}
+
+bool write_geometry(const std::string& path, const Geometry& g, std::string& msg) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) {
+    msg = "cannot write " + path;
+    return false;
+  }
+  std::fprintf(f, "%12zu\n", g.x.size());
+  for (size_t i = 0; i < g.x.size(); i++) std::fprintf(f, " %.17g %.17g %d\n", g.x[i], g.y[i], g.bodyno[i]);
+  bool ok = std::fclose(f) == 0;
+  if (!ok) msg = "write failed: " + path;
+  return ok;
+}
+
+std::vector<std::string> spacing_warnings(const Geometry& g, double ds) {
+  std::vector<std::string> out;
+  std::vector<int> bodies;
+  for (int b : g.bodyno)
+    if (std::find(bodies.begin(), bodies.end(), b) == bodies.end()) bodies.push_back(b);
+  for (int b : bodies) {
+    double lo = 1e300, hi = 0.0;
+    int prev = -1, n = 0;
+    for (size_t i = 0; i < g.x.size(); i++) {
+      if (g.bodyno[i] != b) continue;
+      n++;
+      if (prev >= 0) {
+        const double d = std::hypot(g.x[i] - g.x[prev], g.y[i] - g.y[prev]);
+        lo = std::min(lo, d);
+        hi = std::max(hi, d);
+      }
+      prev = (int)i;
+    }
+    if (n < 2) continue;
+    if (lo < 0.5 * ds || hi > 2.0 * ds) {
+      char m[256];
+      std::snprintf(m, sizeof m,
+                    "WARNING: body %d point spacing %.4g .. %.4g is outside [0.5, 2] x grid spacing %.4g", b, lo, hi,
+                    ds);
+      out.push_back(m);
+    }
+  }
+  return out;
 }
 
 namespace {

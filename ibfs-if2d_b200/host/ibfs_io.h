@@ -45,6 +45,23 @@ bool read_geometry(const std::string& path, Geometry& g, std::string& msg);
 // geom.inp is absent (grid.f90:353, 496-520).
 Geometry default_geometry(const ibfs_params_c& p);
 
+// The reference's geometry primitives (grid.f90:408-520), appended to g:
+//   vertex x y body                one point
+//   line len aoa body              len/ds segments with end points, centred on
+//                                  the origin at -aoa degrees (the reference's
+//                                  line ignores its x, y arguments)
+//   segment x1 y1 x2 y2 body       the len/ds - 1 interior points
+//   circle dia x y body            INT(pi dia / ds) points from angle 0
+// A spec text holds one primitive per line ('#' starts a comment); ds is the
+// grid spacing len/m. Returns false with msg on a malformed line.
+bool geometry_from_spec(const std::string& text, double ds, Geometry& g, std::string& msg);
+bool write_geometry(const std::string& path, const Geometry& g, std::string& msg);
+
+// The check the reference leaves out (grid.f90:280-284): for every body, the
+// distance between consecutive points against ds; one message per body whose
+// spacing leaves [0.5 ds, 2 ds] (the delta function spans 1.5 ds).
+std::vector<std::string> spacing_warnings(const Geometry& g, double ds);
+
 // Fortran unformatted sequential records (gfortran layout: 4-byte
 // little-endian length markers around the payload; payloads above
 // 2147483639 bytes are split into subrecords, the leading marker negative

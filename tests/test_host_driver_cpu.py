@@ -96,3 +96,29 @@ def test_bad_namelist(tmp_path):
     write_inp(tmp_path, "&READ_PARAMETERS M=3.5 /\n")
     rc, out, err = run(tmp_path)
     assert rc != 0 and "bad value" in err
+
+
+def test_geometry_primitives_and_spacing_check(tmp_path):
+    """input/geom.spec builds the body from the reference's primitives
+    (grid.f90:408-520) with the reference's point placement; the point spacing
+    is checked against the grid spacing (the check grid.f90:280-284 asks for)."""
+    import workloads as W
+    write_inp(tmp_path, "&READ_PARAMETERS M=64, N=64, LEN=4.0, OFFSETX=2.0, OFFSETY=2.0 /\n")
+    (tmp_path / "input" / "geom.spec").write_text("# a plate and a cylinder\nline 1.0 30 0\ncircle 0.5 0.2 0.1 1\n")
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    p = json.loads(out)
+    xl, yl = W.line(4.0 / 64, 1.0, 30.0)
+    xc, yc = W.circle(4.0 / 64, 0.5, 0.2, 0.1)
+    assert p["nb"] == len(xl) + len(xc)
+    assert abs(p["x0"] - xl[0]) < 1e-15 and abs(p["y0"] - yl[0]) < 1e-15
+    assert abs(p["xsum"] - (xl.sum() + xc.sum())) < 1e-12 and abs(p["ysum"] - (yl.sum() + yc.sum())) < 1e-12
+    assert "WARNING" not in err
+    # points far apart for the grid: warned, not refused
+    (tmp_path / "input" / "geom.inp").write_text("3\n 0.0 0.0 0\n 0.5 0.0 0\n 1.0 0.0 0\n")
+    rc, out, err = run(tmp_path)
+    assert rc == 0 and "WARNING: body 0 point spacing" in err
+    (tmp_path / "input" / "geom.inp").unlink()
+    (tmp_path / "input" / "geom.spec").write_text("ellipse 1 2 0\n")
+    rc, out, err = run(tmp_path)
+    assert rc != 0 and "unknown primitive" in err
