@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include <mutex>
 #include "../../include/ibfs_capi.h"
 #include "ibfs_handle.cuh"
 
@@ -175,20 +176,92 @@ static double* cos_table(ibfs_handle* h, int m) {
 }
 
 // ---------------------------------------------------------------------------
+// Tile autotuner of the FP64 transform GEMMs. A launch group (the GEMMs of one
+// step-program entry) is timed once with each of the four tile shapes --
+// its outputs redirected to a scratch buffer, its inputs read where they lie,
+// so no state changes -- and the fastest shape is kept. Results are cached
+// per process and device by the group's shape signature, so handles of the
+// same sizes tune once. The tile shape does not change the order of any
+// output's K sum: every shape gives bit-identical results.
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tuned;
+
+static std::string gemm_signature(const std::vector<GemmDesc>& ds, bool dual) {
+  std::vector<std::string> parts;
+  for (auto& d : ds) parts.push_back(std::to_string(d.M) + "x" + std::to_string(d.N) + "x" + std::to_string(d.K) + ":" +
+                                     std::to_string(d.pro) + "/" + std::to_string(d.epi));
+  std::sort(parts.begin(), parts.end());
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::string key = "dev" + std::to_string(dev) + (dual ? "|dual|" : "|");
+  for (auto& p : parts) key += p + ";";
+  return key;
+}
+
+static int tune_gemm(const std::vector<GemmDesc>& ds, bool dual, cudaStream_t st) {
+  const int fallback = [&] {
+    long tiles64 = 0;
+    for (auto& d : ds) tiles64 += gemm_tiles(d.M, d.N, 0);
+    return tiles64 >= 2 * 148 ? 0 : 1;
+  }();
+  const std::string key = gemm_signature(ds, dual);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find(key);
+  if (it != g_tuned.end()) return it->second;
+  size_t need = 1;
+  for (auto& d : ds) need = std::max(need, (size_t)d.ldc * (size_t)d.N);
+  std::vector<GemmDesc> t = ds;
+  double* scratch = nullptr;
+  GemmDesc* dd = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int best = fallback;
+  if (cudaMalloc(&scratch, need * sizeof(double)) == cudaSuccess &&
+      cudaMalloc(&dd, sizeof(GemmDesc) * t.size()) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+      cudaEventCreate(&e1) == cudaSuccess) {
+    for (auto& d : t) {
+      d.C = scratch;
+      if (d.C2) d.C2 = scratch;
+    }
+    cudaMemcpy(dd, t.data(), sizeof(GemmDesc) * t.size(), cudaMemcpyHostToDevice);
+    float best_ms = 1e30f;
+    for (int cfg = 0; cfg < 4; cfg++) {
+      int mt = 0;
+      for (auto& d : t) mt = std::max(mt, gemm_tiles(d.M, d.N, cfg));
+      launch_gemm_f64(dd, (int)t.size(), mt, cfg, dual, st);  // warm-up
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < 3; r++) launch_gemm_f64(dd, (int)t.size(), mt, cfg, dual, st);
+      cudaEventRecord(e1, st);
+      float ms = 0.f;
+      if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
+          ms < best_ms) {
+        best_ms = ms;
+        best = cfg;
+      }
+    }
+  }
+  cudaGetLastError();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (dd) cudaFree(dd);
+  if (scratch) cudaFree(scratch);
+  g_tuned[key] = best;
+  return best;
+}
+
+int tuned_gemm_sites() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return (int)g_tuned.size();
+}
+
+// ---------------------------------------------------------------------------
 // Step program construction
 struct ProgBuilder {
   ibfs_handle* h;
   Prog& P;
   void add(std::function<void()> fn, int tag = TAG_STENCIL, double flops = 0.0) { P.push_back({fn, tag, flops}); }
-  int cfg_for(const std::vector<GemmDesc>& ds) {
-    if (h->tile_cfg >= 0) return h->tile_cfg;
-    long tiles64 = 0;
-    for (auto& d : ds) tiles64 += gemm_tiles(d.M, d.N, 0);
-    return tiles64 >= 2 * 148 ? 0 : 1;
-  }
   void gemm(std::vector<GemmDesc> ds, bool dual) {
     if (ds.empty()) return;
-    int cfg = cfg_for(ds);
+    const int cfg = h->tile_cfg >= 0 ? h->tile_cfg : tune_gemm(ds, dual, h->st);
     int mt = 0;
     for (auto& d : ds) mt = std::max(mt, gemm_tiles(d.M, d.N, cfg));
     GemmDesc* dd = dupload(h, ds);

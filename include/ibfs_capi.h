@@ -60,7 +60,7 @@ typedef struct {
                           grid.f90:523-576); 1: rigid pitching about (pivot_x,pivot_y),
                           alpha(t) = amp*sin(2 pi f t), points move, reg rebuilt        */
   double pitch_amp_deg, pitch_freq, pivot_x, pivot_y;
-  int tile_cfg;        /* transform tile shape; -1 = chosen by the autotuner          */
+  int tile_cfg;        /* FP64 transform tile shape 0..3; -1 = the measured autotuner  */
 } ibfs_options_c;
 
 typedef struct ibfs_handle ibfs_handle;
