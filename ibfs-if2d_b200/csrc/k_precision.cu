@@ -11,16 +11,16 @@
 //     x0 = S f S v        r = v - A x0 (FP64)        x = x0 + S f S r
 // which brings the ~1e-6 error of one split solve down to ~1e-12.
 //
-// GEMM kernel (k_gemm_tc<BN>): one CTA (128 threads) per 128 x BN output
-// tile, BN = 256 (K blocks of 32, 64-byte swizzle, 3 stages of 72 KB) or 128
-// for grids that 256 would pad (K blocks of 64, 128-byte swizzle, 2 stages of
-// 96 KB). Per K block six operand tiles (A0..A2, B0..B2) are brought into
-// swizzled K-major shared memory by TMA (issued by thread 0); thread 32 issues
-// the six slice products as tcgen05.mma (M128 N=BN K16, BF16 in, FP32
-// accumulate in TMEM) and commits to an mbarrier that frees the stage; the
-// four warps read the accumulator back with tcgen05.ld for the epilogue. All
-// mbarrier waits are bounded; a timeout sets an error flag and the CTA frees
-// its TMEM and returns.
+// GEMM kernel (k_gemm_tc_persist): a persistent launch over all 128x128
+// output tiles of all (case, level) GEMMs of one stage, one CTA per SM. Per K
+// block of 64 the six operand tiles (A0..A2, B0..B2, 96 KB) are brought into
+// swizzled K-major shared memory by TMA (two stages, issued by one thread);
+// one thread issues the slice products as tcgen05.mma (M128 N128 K16, BF16 in,
+// FP32 accumulate in TMEM, double-buffered accumulators); eight warps drain
+// them with tcgen05.ld. The 128-wide tile was measured against a 256-wide one
+// with K blocks of 32 (38.8 vs 42.2 ms of GEMM per step of the 256-case batch)
+// and kept. All mbarrier waits are bounded in time; a wait that gives up sets
+// an error status, the CTA frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -210,17 +210,6 @@ struct __align__(64) TcDesc {
   float nu, norm;     // F_LAM1I_NORM: 1/((1 + nu lam) norm); F_LAMINV: 1/(lam norm)
 };
 
-// Tile shapes: 128 x BN outputs, K blocks of BK, STAGES-deep operand ring.
-//   BN = 128: BK = 64 (128 B rows, 128 B swizzle), 2 stages of 96 KB
-//   BN = 256: BK = 32 (64 B rows, 64 B swizzle),   3 stages of 72 KB
-template <int BN> struct TcShape;
-template <> struct TcShape<128> { static constexpr int BK = 64, STAGES = 2; };
-template <> struct TcShape<256> { static constexpr int BK = 32, STAGES = 3; };
-template <int BN> constexpr int tc_a_bytes() { return 128 * TcShape<BN>::BK * 2; }
-template <int BN> constexpr int tc_b_bytes() { return BN * TcShape<BN>::BK * 2; }
-template <int BN> constexpr int tc_stage_bytes() { return 3 * tc_a_bytes<BN>() + 3 * tc_b_bytes<BN>(); }
-template <int BN> constexpr int tc_smem() { return TcShape<BN>::STAGES * tc_stage_bytes<BN>() + 1024 + 256; }
-
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
@@ -256,160 +245,8 @@ __device__ __forceinline__ void store8(bf16* dst, const bf16* v) {
   *reinterpret_cast<uint4*>(dst) = u;
 }
 
-// Warp-specialised: thread 0 issues the TMA loads, thread 32 the tcgen05.mma
-// (six slice products per K block), all four warps run the epilogue from TMEM.
-template <int BN>
-__global__ void __launch_bounds__(128, 1) k_gemm_tc(const TcDesc* __restrict__ descs, int* __restrict__ status) {
-  constexpr int BK = TcShape<BN>::BK, S = TcShape<BN>::STAGES;
-  constexpr int AB = tc_a_bytes<BN>(), BB = tc_b_bytes<BN>(), SB = tc_stage_bytes<BN>();
-  const TcDesc& d = descs[blockIdx.y];
-  if ((int)blockIdx.x >= d.tiles_m * d.tiles_n) return;
-  const int m0 = (blockIdx.x % d.tiles_m) * 128, n0 = (blockIdx.x / d.tiles_m) * BN;
-  extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* bars = (uint64_t*)(smem + S * SB);  // full[S], empty[S], done
-  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + 8 * (2 * S + 1));
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t sbase = smem_u32(smem);
-  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[S]), done = smem_u32(&bars[2 * S]);
-
-  if (warp == 0) tmem_alloc(smem_u32(tmem_slot), BN);
-  if (tid == 0) {
-    for (int b = 0; b < 2 * S + 1; b++) mbar_init(smem_u32(&bars[b]), 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  const int nk = d.Kp / BK;
-  bool to = false;
-
-  if (tid == 0) {
-    asm volatile("prefetch.tensormap [%0];\n" ::"l"((uint64_t)&d.mapA) : "memory");
-    asm volatile("prefetch.tensormap [%0];\n" ::"l"((uint64_t)&d.mapB) : "memory");
-    int issued = 0;
-    for (int kb = 0; kb < nk; kb++) {
-      const int s = kb % S;
-      if (kb >= S && !mbar_spin(empty0 + 8 * s, ((kb / S) + 1) & 1)) { to = true; break; }
-      const uint32_t fb = full0 + 8 * s;
-      mbar_expect_tx(fb, SB);
-      const uint32_t st = sbase + s * SB;
-      for (int t = 0; t < 3; t++) tma_load_3d(st + t * AB, &d.mapA, kb * BK, m0, t, fb);
-      for (int t = 0; t < 3; t++) tma_load_3d(st + 3 * AB + t * BB, &d.mapB, kb * BK, n0, t, fb);
-      issued = kb + 1;
-    }
-    if (to) {  // let the copies already issued land before leaving
-      for (int kb = issued > S ? issued - S : 0; kb < issued; kb++) mbar_wait(full0 + 8 * (kb % S), (kb / S) & 1);
-    }
-  } else if (tid == 32) {
-    const int pa[6] = {0, 0, 1, 0, 1, 2};
-    const int pb[6] = {0, 1, 0, 2, 1, 0};
-    for (int kb = 0; kb < nk; kb++) {
-      const int s = kb % S;
-      if (!mbar_spin(full0 + 8 * s, (kb / S) & 1)) { to = true; break; }
-      tc_fence_after();
-      const uint32_t st = sbase + s * SB;
-#pragma unroll
-      for (int p = 0; p < 6; p++) {
-#pragma unroll
-        for (int k16 = 0; k16 < BK / 16; k16++) {
-          uint64_t da = smem_desc_kmajor<BK>(st + pa[p] * AB + k16 * 32);
-          uint64_t db = smem_desc_kmajor<BK>(st + 3 * AB + pb[p] * BB + k16 * 32);
-          umma_bf16<BN>(tmem, da, db, (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
-        }
-      }
-      umma_commit(empty0 + 8 * s);
-    }
-    if (!to) umma_commit(done);
-  }
-  if (!to && !mbar_wait(done, 0)) to = true;
-  __syncwarp();
-  if (__syncthreads_or(to)) {
-    if (tid == 0) atomicOr(status, 2);
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, BN);
-    return;
-  }
-  tc_fence_after();
-
-  // epilogue: warp w owns tile rows 32w..32w+31 (TMEM lanes), one row per lane.
-  // Descriptor fields go to registers first (stores through Cs / C64 would
-  // otherwise force reloads of every field).
-  const int M = d.M, N = d.N, epi = d.epi, fkind = d.fkind, ldcs = d.ldcs, ldc = d.ldc;
-  const long long sC = d.sC;
-  bf16* const Cs = d.Cs;
-  double* const C64 = d.C64;
-  const float* const lamy = d.lamy;
-  const float nu = d.nu, norm = d.norm;
-  const int i = m0 + warp * 32 + lane;
-  const int r0 = m0 + warp * 32;
-  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-  float* stg = reinterpret_cast<float*>(smem) + warp * (32 * 33);  // stage area is free now
-  float lx = (epi == TC_SCALE_SPLIT_ROW && i < M) ? __ldg(&d.lamx[i]) : 0.f;
-#pragma unroll 1
-  for (int ch = 0; ch < BN / 32; ch++) {
-    float v[32];
-    tmem_ld32(trow + ch * 32, v);
-    const int jb = n0 + ch * 32;
-    if (epi == TC_SPLIT_COL) {
-      // transpose through shared memory: lane l then owns column jb+l, rows r0..r0+31
-#pragma unroll
-      for (int t = 0; t < 32; t++) stg[t * 33 + lane] = v[t];
-      __syncwarp();
-      if (r0 < ldcs) {
-        const int j = jb + lane;
-        bf16 s0[32], s1[32], s2[32];
-#pragma unroll
-        for (int r = 0; r < 32; r++) split3f(stg[lane * 33 + r], s0[r], s1[r], s2[r]);
-        bf16* o = Cs + (size_t)j * ldcs + r0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          store8(o + q * 8, s0 + q * 8);
-          store8(o + sC + q * 8, s1 + q * 8);
-          store8(o + 2 * sC + q * 8, s2 + q * 8);
-        }
-      }
-      __syncwarp();
-    } else if (epi == TC_SCALE_SPLIT_ROW) {
-      if (jb < ldcs) {
-        bf16 s0[32], s1[32], s2[32];
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-          const int j = jb + t;
-          float f = 0.f;
-          if (i < M && j < N) {
-            float lam = lx + __ldg(&lamy[j]);
-            f = fkind == F_LAMINV ? __frcp_rn(lam * norm) : __frcp_rn((1.f + nu * lam) * norm);
-          }
-          split3f(v[t] * f, s0[t], s1[t], s2[t]);
-        }
-        bf16* o = Cs + (size_t)i * ldcs + jb;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          store8(o + q * 8, s0 + q * 8);
-          store8(o + sC + q * 8, s1 + q * 8);
-          store8(o + 2 * sC + q * 8, s2 + q * 8);
-        }
-      }
-    } else if (i < M) {
-#pragma unroll
-      for (int t = 0; t < 32; t++) {
-        const int j = jb + t;
-        if (j < N) {
-          size_t o = (size_t)i + (size_t)j * ldc;
-          C64[o] = epi == TC_F64_ADD ? C64[o] + (double)v[t] : (double)v[t];
-        }
-      }
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, BN);
-}
-
 // ---------------------------------------------------------------------------
-// Persistent form of the same GEMM (k_gemm_tc_persist): one CTA per SM walks
+// Persistent GEMM (k_gemm_tc_persist): one CTA per SM walks
 // a cost-sorted work list of (desc, tile) items. Warp 0 lane 0 issues the TMA
 // loads, warp 1 lane 0 the tcgen05.mma; the accumulator is double-buffered in
 // TMEM (2 x 128 columns) so warps 2-5 drain tile t (tcgen05.ld + epilogue)
@@ -743,7 +580,7 @@ struct CaseBufs {
   CUtensorMap mapX, mapT, mapSm, mapSn;
   const float* lamx;
   const float* lamy;
-  int bn;  // output tile width of this case's GEMMs (128 or 256)
+  int bn;  // output tile width of this case's GEMMs (128)
 };
 
 struct PrecisionPlan {
@@ -755,7 +592,6 @@ struct PrecisionPlan {
 };
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-static bool g_persist = true;  // persistent GEMM (default) or one CTA per tile
 static int g_num_sms = 0;
 
 static inline int rup(int x, int a) { return (x + a - 1) / a * a; }
@@ -774,11 +610,7 @@ static bool make_map(CUtensorMap* map, const bf16* base, int ld, int rows, long 
   return r == CUDA_SUCCESS;
 }
 
-// Tile width for an output dimension N. Measured on B200 (256-case batch):
-// 128-wide tiles with 64-element K blocks (38.8 ms of GEMM per step) beat
-// 256-wide tiles with 32-element K blocks (42.2 ms), so 128 is used; the
-// 256-wide variant stays available to the tile autotuner.
-static int pick_bn(int N) { (void)N; return 128; }
+
 
 // lambda(i) = 2 - 2 cos(pi (i+1) / m) = 4 sin^2(pi (i+1) / 2m), free of cancellation.
 static float* lam_table(PrecisionPlan* pp, int m) {
@@ -834,11 +666,7 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   pp->alloc = alloc;
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<256>()) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_gemm_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, kPSmem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_gemm_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, kPSmem) != cudaSuccess) {
       g_perr = "cannot raise shared memory limit for the tensor-core GEMM";
       return 4;
     }
@@ -846,8 +674,6 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    const char* env = getenv("IBFS_TC_PER_TILE");
-    if (env && env[0] == '1') g_persist = false;
   }
   pp->status = cases.empty() ? (int*)alloc(sizeof(int) * 4) : cases[0].status;
   if (!g_encode) {
@@ -861,8 +687,8 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   }
   for (auto& c : cases) {
     CaseBufs b{};
-    b.bn = pick_bn(c.n - 1);
-    const int bk = b.bn == 256 ? 32 : 64;
+    b.bn = 128;
+    const int bk = 64;
     int Rm = rup(c.m - 1, 128), Rn = rup(c.n - 1, b.bn), Km = rup(c.m - 1, 64), Kn = rup(c.n - 1, 64);
     b.sX = (long long)Rm * Kn;
     b.sT = (long long)Rn * Km;
@@ -935,28 +761,7 @@ static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDes
 }
 
 static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all, cudaStream_t st) {
-  if (g_persist) {
-    add_gemm_persist(pp, P, all, st);
-    return;
-  }
-  for (int bn : {128, 256}) {
-    std::vector<TcDesc> ds;
-    for (auto& d : all) if (d.bn == bn) ds.push_back(d);
-    if (ds.empty()) continue;
-    int mt = 0;
-    double fl = 0.0;
-    for (auto& d : ds) {
-      mt = std::max(mt, d.tiles_m * d.tiles_n);
-      fl += 2.0 * d.M * (double)d.N * (double)(d.epi == TC_SPLIT_COL ? d.N : d.M);  // algorithmic (unpadded) K
-    }
-    TcDesc* dd = upload(pp, ds);
-    int nd = (int)ds.size();
-    int* status = pp->status;
-    if (bn == 128)
-      P.push_back({[=]() { k_gemm_tc<128><<<dim3(mt, nd), 128, tc_smem<128>(), st>>>(dd, status); }, TAG_GEMM_TC, fl});
-    else
-      P.push_back({[=]() { k_gemm_tc<256><<<dim3(mt, nd), 128, tc_smem<256>(), st>>>(dd, status); }, TAG_GEMM_TC, fl});
-  }
+  add_gemm_persist(pp, P, all, st);
 }
 
 static void add_prep(PrecisionPlan* pp, Prog& P, const std::vector<PrepDesc>& ds, cudaStream_t st) {
