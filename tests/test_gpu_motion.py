@@ -101,3 +101,24 @@ def test_pitching_batch_equals_single_handles():
         fo.append(o["fx"][0])
     fb = np.array([g.outputs_of(hist[k], 0)["fx"][0] for k in range(5)])
     assert rel(fb, fo) < 1e-9
+
+
+def test_amplitude_derivative_by_central_differences():
+    """d(mean drag)/d(pitch amplitude) from one batch of A -+ h cases: the
+    central differences at two step sizes agree (O(h^2) truncation), and J (the
+    mean of the two neighbours, O(h^2) from J(A)) is the mean drag of a
+    single-handle run at A within that."""
+    import sensitivity as S
+    kw = dict(m=48, levels=2, re=500.0, dt=0.01, freq=0.25)
+    amps = [10.0, 25.0]
+    J1, g1 = S.mean_drag_amplitude_derivative(amps, h_deg=0.05, steps=12, tail=6, **kw)
+    J2, g2 = S.mean_drag_amplitude_derivative(amps, h_deg=0.025, steps=12, tail=6, **kw)
+    assert np.all(np.abs(g1 - g2) <= 1e-3 * np.abs(g2) + 1e-9)
+    assert np.all(np.abs(J1 - J2) <= 1e-5 * np.abs(J2))
+    import workloads as W
+    c = W.pitching(amp_deg=amps[0], **kw)
+    p, b, o = W.solver_args([c], C)
+    s = C.Solver(p[0], b[0], o[0])
+    h = s.advance_n(12)
+    J = np.mean([s.outputs_of(h[k], 0)["fx"][0] for k in range(6, 12)])
+    assert abs(J2[0] - J) <= 1e-5 * abs(J)
