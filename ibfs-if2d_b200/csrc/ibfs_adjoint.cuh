@@ -21,6 +21,7 @@ struct AdjCase {
   const double* fwQ; // forward q at the start of that step
   const double* wx;  // [nbody] objective weights of the step's forces
   const double* wy;
+  const double* tq;  // [nf][9] (q1 + q0) at each force's faces in that step (moving body)
 };
 
 void adj_curlT(const DevCase* c, const AdjCase* a, const DevCase& h, int nlev, int use_q1, cudaStream_t st);
@@ -31,6 +32,10 @@ void adj_force(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_
 void adj_solve(const DevCase* c, const double* in, double* tmp, double* out, const DevCase& h, cudaStream_t st);
 void adj_rhsf(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st);
 void adj_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, int first, cudaStream_t st);
+void adjm_reg_in(const DevCase* c, const AdjCase* a, const double* x, const DevCase& h, cudaStream_t st);
+void adjm_regT_curl0(const DevCase* c, const AdjCase* a, double* out, const DevCase& h, cudaStream_t st);
+void adjm_position(const DevCase* c, const AdjCase* a, const double* zcg, const double* u, double* acc,
+                   cudaStream_t st);
 void adj_nonlinear(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st);
 
 }  // namespace ibfs

@@ -53,15 +53,15 @@ static void adj_add_v2f(ProgBuilder& B, const DevCase* dc, const AdjCase* da, co
   for (int k = c.L; k >= 2; k--) B.add([=]() { adj_coarsifyT(dc, da, hc, k, st); });
 }
 
-static void adj_build(ibfs_handle* h, AdjPlan& P, Prog& prog, int first) {
+// Adjoint step, first part: steps (7) and (6) of the forward step run
+// backwards, ending with the adjoint of fb (aF).
+static void adj_build_head(ibfs_handle* h, AdjPlan& P, ProgBuilder& B) {
   const DevCase& c = h->cases[0].dc;
   const DevCase* dc = h->d_cases;
   const AdjCase& a = P.a;
   const AdjCase* da = P.d_a;
   cudaStream_t st = h->st;
-  ProgBuilder B{h, prog};
   DevCase hc = c;
-  size_t nsL = (size_t)c.L * c.ns;
   double* aLb = a.aLb;
   size_t lbb = sizeof(double) * c.L * c.nring;
   B.add([=]() { cudaMemsetAsync(aLb, 0, lbb, st); });
@@ -73,9 +73,18 @@ static void adj_build(ibfs_handle* h, AdjPlan& P, Prog& prog, int first) {
   B.gemm({right_desc(c, a.aT2, a.aT1)}, false);
   B.gemm({left_desc(c, a.aT1, a.aZ1, EPI_STORE, 1)}, false);
   B.add([=]() { adj_force(dc, da, hc, st); });
-  // (5) fb = cholsl(rhsf): the factor's solve is symmetric
-  double *aF = a.aF, *aTmp = a.aTmp, *aRf = a.aRf;
-  B.add([=]() { adj_solve(dc, aF, aTmp, aRf, hc, st); }, TAG_CHOL);
+}
+
+// Adjoint step, last part: from the adjoint of rhsf (aRf) through steps (4)
+// to (1).
+static void adj_build_tail(ibfs_handle* h, AdjPlan& P, ProgBuilder& B, int first) {
+  const DevCase& c = h->cases[0].dc;
+  const DevCase* dc = h->d_cases;
+  const AdjCase& a = P.a;
+  const AdjCase* da = P.d_a;
+  cudaStream_t st = h->st;
+  DevCase hc = c;
+  size_t nsL = (size_t)c.L * c.ns;
   // (4) rhsf = regT(q_1) - motion
   B.add([=]() { adj_rhsf(dc, da, hc, st); });
   // (3) vort2flux(q(:,1), omega, 1), operators.f90:163
@@ -110,7 +119,23 @@ static void adj_build(ibfs_handle* h, AdjPlan& P, Prog& prog, int first) {
   B.add([=]() { cudaMemcpyAsync(aW, aW2, sizeof(double) * nsL, cudaMemcpyDeviceToDevice, st); });
 }
 
-static int adj_init(ibfs_handle* h, AdjPlan& P) {
+// The whole adjoint step of a stationary body: (5) fb = cholsl(rhsf) is
+// symmetric, so its adjoint is the same two triangular solves.
+static void adj_build(ibfs_handle* h, AdjPlan& P, Prog& prog, int first) {
+  const DevCase& c = h->cases[0].dc;
+  const DevCase* dc = h->d_cases;
+  const AdjCase& a = P.a;
+  cudaStream_t st = h->st;
+  ProgBuilder B{h, prog};
+  DevCase hc = c;
+  adj_build_head(h, P, B);
+  double *aF = a.aF, *aTmp = a.aTmp, *aRf = a.aRf;
+  B.add([=]() { adj_solve(dc, aF, aTmp, aRf, hc, st); }, TAG_CHOL);
+  adj_build_tail(h, P, B, first);
+}
+
+// Buffers of the adjoint working set of the handle's single case.
+static int adj_alloc(ibfs_handle* h, AdjPlan& P) {
   const DevCase& c = h->cases[0].dc;
   size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
   AdjCase& a = P.a;
@@ -135,8 +160,13 @@ static int adj_init(ibfs_handle* h, AdjPlan& P) {
   a.aGrad = dalloc<double>(h, c.nf);
   P.d_a = dalloc<AdjCase>(h, 1);
   if (!a.aW || !a.aQ || !a.aS || !a.aGrad || !P.d_a) return set_error(IBFS_ERR_NOMEM, "adjoint allocation failed");
-
   P.state = 2 * nsL + nqL + c.nf;
+  return IBFS_OK;
+}
+
+static int adj_init(ibfs_handle* h, AdjPlan& P) {
+  int rc = adj_alloc(h, P);
+  if (rc) return rc;
   adj_build(h, P, P.bw, 0);
   adj_build(h, P, P.bw_first, 1);
   int kk = 0;

@@ -955,9 +955,17 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out);
 }  // namespace ibfs
 
 #include "ibfs_adjoint_host.cuh"
+#include "ibfs_adjoint_motion_host.cuh"
 
 namespace ibfs {
 static void free_adj(ibfs_handle* h) {
+  if (h->adjm) {
+    for (cudaGraphExec_t g : {h->adjm->g_head, h->adjm->g_tail, h->adjm->g_tailf, h->adjm->g_start,
+                              h->adjm->g_iter, h->adjm->g_iter50, h->adjm->g_u})
+      if (g) cudaGraphExecDestroy(g);
+    delete h->adjm;
+    h->adjm = nullptr;
+  }
   if (!h->adj) return;
   if (h->adj->g_bw) cudaGraphExecDestroy(h->adj->g_bw);
   if (h->adj->g_bwf) cudaGraphExecDestroy(h->adj->g_bwf);
@@ -1210,6 +1218,14 @@ int ibfs_adjoint_run(ibfs_handle* h, int nsteps, int checkpoint_every, const dou
                      const double* wy, double* J, double* grad_vel, double* ms_forward, double* ms_total) {
   if (!h) return IBFS_ERR_ARG;
   int rc = adj_run(h, nsteps, checkpoint_every, body_vel, wx, wy, J, grad_vel, ms_forward, ms_total);
+  if (rc) h->err = ibfs_last_error(nullptr);
+  return rc;
+}
+
+int ibfs_adjoint_pitch_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* wx, const double* wy,
+                           double* J, double* dJ_damp, double* ms_forward, double* ms_total) {
+  if (!h) return IBFS_ERR_ARG;
+  int rc = adjm_run(h, nsteps, checkpoint_every, wx, wy, J, dJ_damp, ms_forward, ms_total);
   if (rc) h->err = ibfs_last_error(nullptr);
   return rc;
 }

@@ -64,6 +64,7 @@ struct DevCase {
   int* tface;                    // [Nf][9] face index, ascending
   double* tw;                    // [Nf][9] weight
   double* twsum;                 // [Nf] sum of a force's weights
+  double* tq;                    // [Nf][9] (q + q0) at the force's faces, or null (adjoint capture)
 
   // conjugate gradient (operators.f90:393-441) on the force system
   double *cg_r, *cg_d, *cg_q, *cg_q2;  // [Nf]
@@ -132,6 +133,81 @@ __device__ __forceinline__ double apply_bc_at(double val, int a, int b, int m, i
 
 // lam(i,j) of myfft.f90:131-132 from the cosine tables.
 __device__ __forceinline__ double lam_ij(double ci, double cj) { return -2.0 * (ci + cj - 2.0); }
+
+// ---------------------------------------------------------------------------
+// Immersed-boundary smearing shared by the advance and its adjoint.
+
+// grid.f90:233-249.
+__device__ __forceinline__ double deltafnc_d(double r, double r0, double dr) {
+  double d = fabs(r - r0);
+  if (d <= 0.5 * dr) {
+    double t = (r - r0) / dr;
+    return (1.0 + sqrt(-3.0 * t * t + 1.0)) / (3.0 * dr);
+  } else if (d <= 1.5 * dr) {
+    double a = fabs((r - r0) / dr);
+    double u = 1.0 - a;
+    return (5.0 - 3.0 * a - sqrt(-3.0 * u * u + 1.0)) / (6.0 * dr);
+  }
+  return 0.0;
+}
+
+// d/d r0 of deltafnc_d(r, r0, dr): with t = (r - r0)/dr and deltafnc = psi(t)/dr,
+// psi'(t) = -t / sqrt(1 - 3t^2) on |t| <= 1/2 and
+// -sgn(t) (1 + (1-|t|) / sqrt(1 - 3(1-|t|)^2)) / 2 on 1/2 < |t| <= 3/2
+// (continuous at both joins, zero at |t| = 3/2), so d/dr0 = -psi'(t) / dr^2.
+__device__ __forceinline__ double ddeltafnc_dr0(double r, double r0, double dr) {
+  double d = fabs(r - r0);
+  double t = (r - r0) / dr;
+  double dpsi;
+  if (d <= 0.5 * dr) {
+    dpsi = -t / sqrt(-3.0 * t * t + 1.0);
+  } else if (d <= 1.5 * dr) {
+    double u = 1.0 - fabs(t);
+    dpsi = -copysign(1.0, t) * 0.5 * (1.0 + u / sqrt(-3.0 * u * u + 1.0));
+  } else {
+    return 0.0;
+  }
+  return -dpsi / (dr * dr);
+}
+
+// reg (operators.f90:513-528) at one face: stationary bodies gather from the
+// CSR-by-face table whose entries keep the reference's smear order; moving
+// bodies from the patch tables rebuilt every step.
+__device__ __forceinline__ double reg_face(const DevCase& C, const double* __restrict__ f, int face) {
+  if (C.moving) {  // patch tables rebuilt every step
+    int m = C.m, nu = (m + 1) * C.n, pidx;
+    if (face < nu) {
+      int i = face % (m + 1) + 1 - C.pu_i0, j = face / (m + 1) + 1 - C.pu_j0;
+      if (i < 0 || j < 0 || i >= C.pu_w || j >= C.pu_h) return 0.0;
+      pidx = i + j * C.pu_w;
+    } else {
+      int fv = face - nu;
+      int i = fv % m + 1 - C.pv_i0, j = fv / m + 1 - C.pv_j0;
+      if (i < 0 || j < 0 || i >= C.pv_w || j >= C.pv_h) return 0.0;
+      pidx = C.pu_w * C.pu_h + i + j * C.pv_w;
+    }
+    double h = 0.0;
+    for (int p = 0; p < C.pcnt[pidx]; p++) h = h + C.pw[pidx * kPatchCap + p] * f[C.pf[pidx * kPatchCap + p]];
+    return h;
+  }
+  int p0 = C.face_ptr[face], p1 = C.face_ptr[face + 1];
+  double h = 0.0;
+  for (int p = p0; p < p1; p++) h = h + C.face_w[p] * f[C.face_f[p]];
+  return h;
+}
+
+// regT (operators.f90:531-546) for one force: its faces in ascending order.
+__device__ __forceinline__ double regT_force(const DevCase& C, const double* __restrict__ h, int f) {
+  if (C.moving) {
+    double s = 0.0;
+    for (int p = 0; p < C.tcnt[f]; p++) s = s + C.tw[f * 9 + p] * h[C.tface[f * 9 + p]];
+    return s;
+  }
+  int p0 = C.force_ptr[f], p1 = C.force_ptr[f + 1];
+  double s = 0.0;
+  for (int p = p0; p < p1; p++) s = s + C.force_w[p] * h[C.force_face[p]];
+  return s;
+}
 
 }  // namespace ibfs
 

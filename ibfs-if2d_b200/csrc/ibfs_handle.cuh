@@ -14,7 +14,8 @@
 
 namespace ibfs {
 
-struct AdjPlan;  // adjoint driver state (ibfs_adjoint_host.cuh)
+struct AdjPlan;   // adjoint driver state (ibfs_adjoint_host.cuh)
+struct AdjMPlan;  // moving-body adjoint state (ibfs_adjoint_motion_host.cuh)
 
 struct HostCase {
   ibfs_params_c p;
@@ -78,6 +79,7 @@ struct ibfs_handle {
   int sum_nf = 0;
   double* d_vertex = nullptr;  // 5 x max_ns, vertex fields of the Tecplot export (allocated on first use)
   AdjPlan* adj = nullptr;
+  AdjMPlan* adjm = nullptr;
 };
 
 

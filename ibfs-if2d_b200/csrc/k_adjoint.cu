@@ -180,37 +180,44 @@ __global__ void k_adj_zero_centre(const DevCase* __restrict__ cases, const AdjCa
   A.aW[(size_t)(k - 1) * C.ns + nidx(i, j, m)] = 0.0;
 }
 
+// curl(x, 0) at one face (rot^T of a node field, operators.f90:243-288 with a
+// zero ring).
+__device__ __forceinline__ double curl0_face(const double* __restrict__ x, int m, int n, int face) {
+  auto X = [&](int i, int j) { return (i >= 2 && i <= m && j >= 2 && j <= n) ? x[nidx(i, j, m)] : 0.0; };
+  int nu = (m + 1) * n;
+  if (face < nu) {
+    int i = face % (m + 1) + 1, j = face / (m + 1) + 1;
+    return (i == 1 || i == m + 1) ? 0.0 : X(i, j + 1) - X(i, j);
+  }
+  int fv = face - nu, i = fv % m + 1, j = fv / m + 1;
+  return (j == 1 || j == n + 1) ? 0.0 : X(i, j) - X(i + 1, j);
+}
+
+// regT(curl(x, 0)) for one force, gathered over the force's faces.
+__device__ __forceinline__ double regT_curl0(const DevCase& C, const double* __restrict__ x, int f) {
+  double s = 0.0;
+  if (C.moving) {
+    for (int p = 0; p < C.tcnt[f]; p++) s += C.tw[f * 9 + p] * curl0_face(x, C.m, C.n, C.tface[f * 9 + p]);
+    return s;
+  }
+  for (int q = C.force_ptr[f]; q < C.force_ptr[f + 1]; q++) s += C.force_w[q] * curl0_face(x, C.m, C.n, C.force_face[q]);
+  return s;
+}
+
 // F_hat' = objective term + (-regT(curl0(aZ1))) (projection adjoint,
 // operators.f90:174) ; objective: J += wx_b fx_b + wy_b fy_b with
-// f = 2 delta / dt * sum wsum_f fb_f (write_force).
+// f = 2 delta / dt * sum wsum_f fb_f (write_force; a moving body's wsum is
+// the sum of its current weights).
 __global__ void k_adj_force(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj) {
   const DevCase& C = cases[0];
   const AdjCase& A = adj[0];
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= C.nf) return;
-  int m = C.m, n = C.n;
   int p = f < C.nb ? f : f - C.nb;
   int b = C.bdyno[p] - C.bmin;
   double w = f < C.nb ? A.wx[b] : A.wy[b];
-  double v = w * 2.0 * C.delta / C.dt * C.wsum[f];
-  // regT of curl(x, 0) (x = aZ1, nodes), gathered over the force's faces
-  const double* x = A.aZ1;
-  auto X = [&](int i, int j) { return (i >= 2 && i <= m && j >= 2 && j <= n) ? x[nidx(i, j, m)] : 0.0; };
-  double s = 0.0;
-  for (int q = C.force_ptr[f]; q < C.force_ptr[f + 1]; q++) {
-    int face = C.force_face[q];
-    double cv;
-    int nu = (m + 1) * n;
-    if (face < nu) {
-      int i = face % (m + 1) + 1, j = face / (m + 1) + 1;
-      cv = (i == 1 || i == m + 1) ? 0.0 : X(i, j + 1) - X(i, j);
-    } else {
-      int fv = face - nu, i = fv % m + 1, j = fv / m + 1;
-      cv = (j == 1 || j == n + 1) ? 0.0 : X(i, j) - X(i + 1, j);
-    }
-    s += C.force_w[q] * cv;
-  }
-  A.aF[f] = v - s;
+  double v = w * 2.0 * C.delta / C.dt * (C.moving ? C.twsum[f] : C.wsum[f]);
+  A.aF[f] = v - regT_curl0(C, A.aZ1, f);
 }
 
 // y = Linv b (lower) / x = LinvT y (upper) on adjoint vectors; warp per row.
@@ -234,13 +241,105 @@ __global__ void k_adj_rhsf(const DevCase* __restrict__ cases, const AdjCase* __r
   const DevCase& C = cases[0];
   const AdjCase& A = adj[0];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < C.nq) {
-    int p0 = C.face_ptr[t], p1 = C.face_ptr[t + 1];
-    double h = 0.0;
-    for (int p = p0; p < p1; p++) h = h + C.face_w[p] * A.aRf[C.face_f[p]];
-    A.aQ1[t] = h;
-  }
+  if (t < C.nq) A.aQ1[t] = reg_face(C, A.aRf, t);
   if (t < C.nf) A.aGrad[t] -= C.delta * A.aRf[t];
+}
+
+// ---------------------------------------------------------------------------
+// Moving body (rigid pitching, CG force solve). The force operator
+// A = regT M reg (M = curl vort2flux_1 ainv rot, a_times, operators.f90:444-462)
+// is solved by CG in the forward step; its adjoint needs A^T = regT M^T reg,
+// applied with the transposed operators above, and the derivative of the
+// smearing weights with respect to the body positions.
+
+// aQ1 = reg(x) on all faces (the first operator of A^T).
+__global__ void k_adjm_reg_in(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
+                              const double* __restrict__ x) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < C.nq) A.aQ1[t] = reg_face(C, x, t);
+}
+
+// out = regT(curl(aZ1, 0)) (the last two operators of A^T).
+__global__ void k_adjm_regT_curl0(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
+                                  double* __restrict__ out) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < C.nf) out[f] = regT_curl0(C, A.aZ1, f);
+}
+
+// One step's contribution to dJ/d(pitch amplitude, radians), added to *acc.
+// The weight w(face, f) = dx^2 delta(x_face - X_k) delta(y_face - Y_k) of force
+// f (component of body point k) enters the step through
+//   rhsf  = regT(q1 + q0) - dx V          (b-hat = rhsf_hat = aRf)
+//   fb    = A^-1 rhsf, A = regT M reg     (u = M reg fb, v = M^T reg b-hat)
+//   omega_1 -= ainv rot reg fb            (g = curl0(ainv omega_1-hat) = curl0(aZ1))
+//   fx_b  = 2 dx / dt sum_f fb_f sum_face w(face, f)
+// so dJ/dw(face, f) = b-hat_f (q1 + q0 - u)_face - fb_f (g + v)_face
+//                     + 2 dx / dt wobj_f fb_f,
+// and dJ/dX_k = sum over both components and their faces of dw/dX_k times it.
+// With alpha = A sin(Om t), theta = -alpha about the pivot:
+//   dX/dA = (Y - py) sin(Om t), dY/dA = -(X - px) sin(Om t),
+//   V = thetadot (-(Y - py), X - px), thetadot = -A Om cos(Om t),
+//   dV/dA from both d thetadot/dA = -Om cos(Om t) and dX/dA, dY/dA;
+// the velocity enters rhsf as -dx V, so dJ/dV_f = -dx b-hat_f.
+// One block; the points are reduced in a fixed order.
+__global__ void k_adjm_position(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
+                                const double* __restrict__ zcg, const double* __restrict__ u,
+                                double* __restrict__ acc) {
+  const DevCase& C = cases[0];
+  const AdjCase& A = adj[0];
+  const int m = C.m, n = C.n, nb = C.nb;
+  const double dx = C.delta, d2 = 0.5 * dx;
+  const double t = C.dt * (double)(*C.itime);
+  const double sn = sin(C.pitch_omega * t), cs = cos(C.pitch_omega * t);
+  const double thd = -C.pitch_amp * C.pitch_omega * cs;
+  double part = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    const double X = C.xb[k], Y = C.yb[k];
+    const int b = C.bdyno[k] - C.bmin;
+    double gx = 0.0, gy = 0.0;
+    for (int comp = 0; comp < 2; comp++) {
+      const int f = comp ? nb + k : k;
+      const double sx = comp ? d2 : 0.0, sy = comp ? 0.0 : d2;
+      const double fbf = C.fb[f], bh = A.aRf[f];
+      const double wobj = (comp ? A.wy[b] : A.wx[b]) * 2.0 * dx / C.dt * fbf;
+      for (int p = 0; p < C.tcnt[f]; p++) {
+        const int face = C.tface[f * 9 + p];
+        int i, j;
+        if (!comp) {
+          i = face % (m + 1) + 1;
+          j = face / (m + 1) + 1;
+        } else {
+          int fv = face - (m + 1) * n;
+          i = fv % m + 1;
+          j = fv / m + 1;
+        }
+        const double x = dx * (double)(i - 1) - C.offx + sx;
+        const double y = dx * (double)(j - 1) - C.offy + sy;
+        const double G = bh * (A.tq[f * 9 + p] - u[face]) -
+                         fbf * (curl0_face(A.aZ1, m, n, face) + curl0_face(zcg, m, n, face)) + wobj;
+        const double px = deltafnc_d(x, X, dx), py = deltafnc_d(y, Y, dx);
+        gx += (dx * dx) * ddeltafnc_dr0(x, X, dx) * py * G;
+        gy += (dx * dx) * px * ddeltafnc_dr0(y, Y, dx) * G;
+      }
+    }
+    const double rx = X - C.pivot_x, ry = Y - C.pivot_y;
+    const double dXdA = ry * sn, dYdA = -rx * sn;
+    const double dVx = C.pitch_omega * cs * ry + thd * rx * sn;
+    const double dVy = -C.pitch_omega * cs * rx + thd * ry * sn;
+    part += gx * dXdA + gy * dYdA - dx * (A.aRf[k] * dVx + A.aRf[nb + k] * dVy);
+  }
+  __shared__ double red[128];
+  red[threadIdx.x] = part;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *acc += red[0];
 }
 
 // Level-k CN adjoint, node part: r_hat = con1 A_hat + P_hat' ; P_hat = con2 A_hat
@@ -367,6 +466,16 @@ void adj_solve(const DevCase* c, const double* in, double* tmp, double* out, con
 }
 void adj_rhsf(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st) {
   k_adj_rhsf<<<(h.nq + 255) / 256, 256, 0, st>>>(c, a);
+}
+void adjm_reg_in(const DevCase* c, const AdjCase* a, const double* x, const DevCase& h, cudaStream_t st) {
+  k_adjm_reg_in<<<(h.nq + 255) / 256, 256, 0, st>>>(c, a, x);
+}
+void adjm_regT_curl0(const DevCase* c, const AdjCase* a, double* out, const DevCase& h, cudaStream_t st) {
+  k_adjm_regT_curl0<<<(h.nf + 127) / 128, 128, 0, st>>>(c, a, out);
+}
+void adjm_position(const DevCase* c, const AdjCase* a, const double* zcg, const double* u, double* acc,
+                   cudaStream_t st) {
+  k_adjm_position<<<1, 128, 0, st>>>(c, a, zcg, u, acc);
 }
 void adj_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, int first, cudaStream_t st) {
   k_adj_level<<<(h.ns + h.nring + 255) / 256, 256, 0, st>>>(c, a, k, first);

@@ -14,20 +14,6 @@
 
 namespace ibfs {
 
-// grid.f90:233-249.
-__device__ __forceinline__ double deltafnc_d(double r, double r0, double dr) {
-  double d = fabs(r - r0);
-  if (d <= 0.5 * dr) {
-    double t = (r - r0) / dr;
-    return (1.0 + sqrt(-3.0 * t * t + 1.0)) / (3.0 * dr);
-  } else if (d <= 1.5 * dr) {
-    double a = fabs((r - r0) / dr);
-    double u = 1.0 - a;
-    return (5.0 - 3.0 * a - sqrt(-3.0 * u * u + 1.0)) / (6.0 * dr);
-  }
-  return 0.0;
-}
-
 // Rigid pitching about (pivot_x, pivot_y): the body is the zero-pitch shape
 // turned by -alpha(t) (the sign convention of line(), grid.f90:442), with
 // alpha(t) = amp sin(omega t), t = itime dt; body velocity = rotation rate x r.

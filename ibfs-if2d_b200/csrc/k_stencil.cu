@@ -179,29 +179,6 @@ __global__ void __launch_bounds__(256) k_curl(const DevCase* __restrict__ cases,
 // vort = rot(reg(fb)) on level 1 (operators.f90:174 / :457, reg :513-528,
 // rot :291-304). reg is gathered per face from the CSR-by-face table whose
 // entries keep the reference's smear order.
-__device__ __forceinline__ double reg_face(const DevCase& C, const double* __restrict__ f, int face) {
-  if (C.moving) {  // patch tables rebuilt every step
-    int m = C.m, nu = (m + 1) * C.n, pidx;
-    if (face < nu) {
-      int i = face % (m + 1) + 1 - C.pu_i0, j = face / (m + 1) + 1 - C.pu_j0;
-      if (i < 0 || j < 0 || i >= C.pu_w || j >= C.pu_h) return 0.0;
-      pidx = i + j * C.pu_w;
-    } else {
-      int fv = face - nu;
-      int i = fv % m + 1 - C.pv_i0, j = fv / m + 1 - C.pv_j0;
-      if (i < 0 || j < 0 || i >= C.pv_w || j >= C.pv_h) return 0.0;
-      pidx = C.pu_w * C.pu_h + i + j * C.pv_w;
-    }
-    double h = 0.0;
-    for (int p = 0; p < C.pcnt[pidx]; p++) h = h + C.pw[pidx * kPatchCap + p] * f[C.pf[pidx * kPatchCap + p]];
-    return h;
-  }
-  int p0 = C.face_ptr[face], p1 = C.face_ptr[face + 1];
-  double h = 0.0;
-  for (int p = p0; p < p1; p++) h = h + C.face_w[p] * f[C.face_f[p]];
-  return h;
-}
-
 __device__ __forceinline__ void regrot_at(const DevCase& C, int t) {
   int m = C.m, n = C.n;
   int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
@@ -252,18 +229,6 @@ void launch_vertex(const DevCase* cases, int c, int k, int ns, double* out, cuda
 
 // regT (operators.f90:531-546) of one face field, gathered per force in the
 // reference's scatter order (ascending face index).
-__device__ __forceinline__ double regT_force(const DevCase& C, const double* __restrict__ h, int f) {
-  if (C.moving) {
-    double s = 0.0;
-    for (int p = 0; p < C.tcnt[f]; p++) s = s + C.tw[f * 9 + p] * h[C.tface[f * 9 + p]];
-    return s;
-  }
-  int p0 = C.force_ptr[f], p1 = C.force_ptr[f + 1];
-  double s = 0.0;
-  for (int p = p0; p < p1; p++) s = s + C.force_w[p] * h[C.force_face[p]];
-  return s;
-}
-
 // motion = body velocity * delta - regT(q0(:,1));  rhsf = regT(q(:,1)) - motion
 // (operators.f90:142-164, grid.f90:573-574).
 __global__ void k_rhsf(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
@@ -273,6 +238,11 @@ __global__ void k_rhsf(const DevCase* __restrict__ cases, const int* __restrict_
   double mot = (C.bvel ? C.bvel[f] * C.delta : 0.0) - regT_force(C, C.q0, f);
   C.motion[f] = mot;
   C.rhsf[f] = regT_force(C, C.q, f) - mot;
+  if (C.tq)  // (q + q0) at the force's faces, kept for the moving-body adjoint
+    for (int p = 0; p < C.tcnt[f]; p++) {
+      int fc = C.tface[f * 9 + p];
+      C.tq[f * 9 + p] = C.q[fc] + C.q0[fc];
+    }
 }
 
 // a_times output column: out = regT(q(:,1)) (operators.f90:461).

@@ -25,7 +25,7 @@ EXPORTS = [
     "ibfs_set_state", "ibfs_get_state", "ibfs_set_cholesky", "ibfs_get_cholesky", "ibfs_precompute",
     "ibfs_advance", "ibfs_advance_n", "ibfs_batch_advance", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
-    "ibfs_last_cg_iterations", "ibfs_adjoint_run", "ibfs_vertex_fields",
+    "ibfs_last_cg_iterations", "ibfs_adjoint_run", "ibfs_adjoint_pitch_run", "ibfs_vertex_fields",
     "ibfs_last_error",
 ]
 
@@ -92,6 +92,7 @@ def lib():
         L.ibfs_kernels_per_step.argtypes = [vp]
         L.ibfs_last_cg_iterations.argtypes = [vp]
         L.ibfs_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
+        L.ibfs_adjoint_pitch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
         L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
@@ -259,6 +260,19 @@ class Solver:
                                            ctypes.byref(J), _p(grad), ctypes.byref(ms_f), ctypes.byref(ms_t)))
         self.itime.value += nsteps
         return J.value, grad, ms_f.value, ms_t.value
+
+    def adjoint_pitch_run(self, nsteps, checkpoint_every, wx, wy):
+        """J and dJ/d(pitch amplitude, per degree) over nsteps advances of a
+        single pitching case (see ibfs_adjoint_pitch_run)."""
+        wx = np.ascontiguousarray(wx, dtype=np.float64)
+        wy = np.ascontiguousarray(wy, dtype=np.float64)
+        J, dJ = ctypes.c_double(), ctypes.c_double()
+        ms_f, ms_t = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().ibfs_adjoint_pitch_run(self.h, nsteps, checkpoint_every, _p(wx), _p(wy), ctypes.byref(J),
+                                                 ctypes.byref(dJ), ctypes.byref(ms_f), ctypes.byref(ms_t)),
+                    step=True)
+        self.itime.value += nsteps
+        return J.value, dJ.value, ms_f.value, ms_t.value
 
     def last_cg_iterations(self):
         return lib().ibfs_last_cg_iterations(self.h)

@@ -176,6 +176,25 @@ int ibfs_kernels_per_step(const ibfs_handle* h);
 int ibfs_adjoint_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* body_vel, const double* wx,
                      const double* wy, double* J, double* grad_vel, double* ms_forward, double* ms_total);
 
+/* Discrete adjoint of nsteps advances of a single rigidly pitching body (no
+ * reference counterpart): motion_kind 1, stationary = .FALSE. (CG force
+ * solve, cjgr operators.f90:393-441), plain FP64 form. From the current state
+ * it runs nsteps advances and returns J = sum_s sum_b (wx[s*nbody+b] fx_b^s +
+ * wy[s*nbody+b] fy_b^s) and dJ_damp = dJ / d(pitch_amp_deg), per degree of
+ * amplitude. The amplitude moves the body points (the regularisation weights
+ * of reg/regT, setup_reg grid.f90:142-230, differentiated through the
+ * Roma-Peskin-Berger kernel, grid.f90:233-249) and sets their velocities
+ * (the right-hand side of the force system). The CG solve is differentiated
+ * as an exact solve: its adjoint is a CG solve with the transposed force
+ * operator, stopped by the same tolerance rule. Checkpoints every
+ * checkpoint_every steps as ibfs_adjoint_run. On return the state is the
+ * state after the nsteps advances; ibfs_last_cg_iterations reports the
+ * largest adjoint CG iteration count. Returns IBFS_ERR_CG_MAXITER (a
+ * warning, results valid) when a forward or adjoint solve used
+ * cg_max_iter iterations. */
+int ibfs_adjoint_pitch_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* wx, const double* wy,
+                           double* J, double* dJ_damp, double* ms_forward, double* ms_total);
+
 /* CG iterations of the last advance (largest over the handle's cases), as
  * cjgr reports them (operators.f90:439-440); 0 for Cholesky handles. */
 int ibfs_last_cg_iterations(const ibfs_handle* h);

@@ -145,3 +145,100 @@ def mean_lift_derivative(m, lev, dt, re, xb, yb, vel, dvel, steps, tail, h=1e-30
         if s >= steps - tail:
             J = J + o["fy"] / tail
     return J.real, J.imag / h
+
+
+def deltafnc_c(r, r0, dr):
+    """grid.f90:233-249 continued analytically to complex positions: the branch
+    is chosen by the real part and |t| becomes sgn(Re t) t, so the complex
+    step carries the derivative of the kernel (C1 at both joins)."""
+    t = (r - r0) / dr
+    d = np.abs(t.real)
+    a = np.where(t.real >= 0.0, t, -t)
+    out = np.zeros(np.shape(t), complex)
+    m1 = d <= 0.5
+    m2 = (~m1) & (d <= 1.5)
+    out[m1] = (1.0 + np.sqrt(-3.0 * t[m1] ** 2 + 1.0)) / (3.0 * dr)
+    out[m2] = (5.0 - 3.0 * a[m2] - np.sqrt(-3.0 * (1.0 - a[m2]) ** 2 + 1.0)) / (6.0 * dr)
+    return out
+
+
+class PitchCplxCase(CplxCase):
+    """Moving body with complex positions: the regularisation is rebuilt from
+    them every step (setup_reg, grid.f90:142-230, box test on the real part)
+    and the force system is solved exactly (dense A from a_times columns),
+    the limit of the CG solve (cjgr) the GPU runs to a relative 1e-12."""
+
+    def set_body(self, xb, yb):
+        m, n, d = self.m, self.n, self.delta
+        xb = np.asarray(xb, complex)
+        yb = np.asarray(yb, complex)
+        self.xb, self.yb = xb.copy(), yb.copy()
+        sup = 1.5 * d
+        E = np.zeros((self.nf, self.nq), complex)
+        iu, ju = np.meshgrid(np.arange(1, m + 2), np.arange(1, n + 1), indexing="ij")
+        xu = d * (iu - 1) - self.offx
+        yu = d * (ju - 1) - self.offy + 0.5 * d
+        idx_u = (iu + (ju - 1) * (m + 1) - 1)
+        iv, jv = np.meshgrid(np.arange(1, m + 1), np.arange(1, n + 2), indexing="ij")
+        xv = d * (iv - 1) - self.offx + 0.5 * d
+        yv = d * (jv - 1) - self.offy
+        idx_v = ((m + 1) * n + iv + (jv - 1) * m - 1)
+        for k in range(self.nb):
+            mk = (np.abs(xu - xb[k].real) < sup) & (np.abs(yu - yb[k].real) < sup)
+            E[k, idx_u[mk]] = d * d * deltafnc_c(xu[mk], xb[k], d) * deltafnc_c(yu[mk], yb[k], d)
+            mk = (np.abs(xv - xb[k].real) < sup) & (np.abs(yv - yb[k].real) < sup)
+            E[self.nb + k, idx_v[mk]] = d * d * deltafnc_c(xv[mk], xb[k], d) * deltafnc_c(yv[mk], yb[k], d)
+        self.E = E
+
+    def step(self, xb, yb, vel):
+        """One advance with the body at (xb, yb) moving at vel (operators.f90:62-188)."""
+        if self.itime == 0:
+            self.make_complex()
+        self.itime += 1
+        L = self.L
+        cz = np.zeros(2 * (self.m + 1) + 2 * (self.n + 1), complex)
+        lastbc = [self.get_bc(self.omega[k + 1], 0.25) for k in range(L - 1)] + [cz]
+        for k in range(L - 1, -1, -1):
+            obc = self.get_bc(self.omega[k + 1], 0.25) if k < L - 1 else cz
+            rhs = self.rot(self.nonlinear(self.omega[k], self.q[k], self.q0[k], lastbc[k]))
+            if self.itime == 1:
+                self.rhs_old[k] = rhs
+            rb = self.apply_bc(np.zeros_like(rhs), lastbc[k], self.vfac[k])
+            rb = self.apply_bc(rb, obc, self.vfac[k])
+            t1 = self.dst(self.con1[k] * rhs + self.con2[k] * self.rhs_old[k] + rb)
+            self.omega[k] = self.dst(self.lam1i[k] * (t1 + self.lam1[k] * self.dst(self.omega[k])))
+            self.rhs_old[k] = rhs
+        self.set_body(xb, yb)
+        motion = np.asarray(vel) * self.delta - self.regT(self.q0[0])
+        vel1 = self.vort2flux(self.omega, 1)
+        rhsf = self.regT(vel1[0]) - motion
+        A = np.stack([self.a_times(e) for e in np.eye(self.nf)], axis=1)
+        self.fb = np.linalg.solve(A, rhsf)
+        self.omega[0] = self.omega[0] - self.ainv(self.rot(self.reg(self.fb)))
+        self.q = self.vort2flux(self.omega, L)
+        h = self.reg(self.fb / self.dt)
+        return dict(fx=h[:self.nu].sum() * 2.0 * self.delta, fy=h[self.nu:].sum() * 2.0 * self.delta)
+
+
+def mean_drag_amplitude_derivative(m, lev, dt, re, xb0, yb0, amp_deg, freq, steps, tail, h=1e-30,
+                                   px=0.0, py=0.0):
+    """J = mean drag over the last `tail` of `steps` advances of a plate pitching
+    as alpha(t) = A sin(2 pi freq t) about (px, py) (the body turned by -alpha),
+    and dJ/dA per degree, by complex step in A."""
+    c = PitchCplxCase(m, m, dt, re, lev, xb0, yb0, stationary=False)
+    A = (amp_deg + 1j * h) * np.pi / 180.0
+    om = 2.0 * np.pi * freq
+    J = 0.0
+    for s in range(1, steps + 1):
+        t = s * dt
+        th = -A * np.sin(om * t)
+        thd = -A * om * np.cos(om * t)
+        cs, sn = np.cos(th), np.sin(th)
+        rx, ry = np.asarray(xb0) - px, np.asarray(yb0) - py
+        x = px + cs * rx - sn * ry
+        y = py + sn * rx + cs * ry
+        vel = np.concatenate([-thd * (y - py), thd * (x - px)])
+        o = c.step(x, y, vel)
+        if s > steps - tail:
+            J = J + o["fx"] / tail
+    return J.real, J.imag / h
