@@ -28,8 +28,9 @@ plate at 30 deg (Re 300, dt 0.002; L2 flushed between steps) and its ratio to
 the headline, the batched FP64 advance of the same 256 cases, the split-vs-FP64
 force and field errors, a sequential sample (cases one handle at a time), the
 split-precision plate, the adjoint/forward cost on the rotating cylinder
-(Re 150, 256x256x4, 126 points), and 32 pitching plates advanced together
-(512x512x5, CG force solve every step).
+(Re 150, 256x256x4, 126 points), 32 pitching plates advanced together
+(512x512x5, CG force solve every step), and the adjoint/forward cost of the
+mean-drag derivative w.r.t. the pitch amplitude on one such plate.
 
 `--impl reference` times the CPU restatement of the reference (the oracle, a
 port: the Fortran+FFTW reference cannot be built here) on all host cores, one
@@ -292,6 +293,32 @@ def pitching_batch(C, steps=3, warmup=2):
     return out
 
 
+def pitch_adjoint_cost(C, steps=12, K=6, amp=20.0):
+    """Config-5 grid (plate pitching about mid-chord, Re 500, 512x512 cells x 5
+    levels, dt 0.001, FP64 CG to a relative 1e-12): the discrete adjoint of the
+    mean drag over the last half of the horizon w.r.t. the pitch amplitude;
+    cost = device time of the gradient run / device time of a plain forward
+    run of the same steps from the same state."""
+    case = W.pitching(amp_deg=amp)
+    p, b, o = W.solver_args([case], C)
+    f = C.Solver(p[0], b[0], o[0])
+    f.advance_n(steps, want_hist=False)
+    ms_plain = f.last_ms()
+    f.close()
+    g = C.Solver(p[0], b[0], o[0])
+    wx = np.zeros(steps)
+    wx[steps - steps // 2:] = 1.0 / (steps // 2)
+    J, dJ, mf, mt = g.adjoint_pitch_run(steps, K, wx, np.zeros(steps))
+    it = g.last_cg_iterations()
+    g.close()
+    return {"cost_ratio": mt / ms_plain, "cost_ratio_vs_own_forward_pass": mt / mf, "ms_total": mt,
+            "ms_forward_pass": mf, "ms_plain_forward": ms_plain, "steps": steps, "checkpoint_every": K,
+            "J": J, "dJ_damp_per_deg": dJ, "adjoint_cg_iterations_max": it,
+            "workload": f"plate pitching {amp} deg about mid-chord, f 0.25, Re 500, 512x512 cells x 5 levels, "
+                        f"dt 0.001, FP64 CG to relative 1e-12; J = mean drag over the last {steps // 2} steps, "
+                        "derivative w.r.t. the pitch amplitude"}
+
+
 def adjoint_cost(C, steps=100, K=50):
     """Rotating cylinder (Re 150, 256x256x4, 126 points, dt .004): the discrete
     adjoint of the mean lift over the last third of the horizon w.r.t. the
@@ -444,6 +471,7 @@ def run_ours(args):
             extras["plate400_split"] = split
             extras["adjoint"] = adjoint_cost(C)
             extras["pitching_batch"] = pitching_batch(C)
+            extras["pitch_adjoint"] = pitch_adjoint_cost(C)
             cpu = cpu_sample_from_gpu(g, cases, sorted(int(x) for x in np.random.default_rng(SEED + 2).choice(
                 ncase, 6, replace=False)), args.cpu_steps)
         out = {

@@ -196,6 +196,7 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
                    double* J, double* grad, double* ms_fwd, double* ms_total) {
   if (h->cases.size() != 1 || !h->cases[0].p.stationary || h->precision != 0)
     return set_error(IBFS_ERR_ARG, "the adjoint needs a single stationary case in the plain FP64 form");
+  if (h->cases[0].dc.nact) return set_error(IBFS_ERR_ARG, "the adjoint does not cover actuator jets");
   if (nsteps < 1 || K < 1 || !wx || !wy || !J || !grad) return set_error(IBFS_ERR_ARG, "bad adjoint arguments");
   HostCase& hc = h->cases[0];
   const DevCase& c = hc.dc;

@@ -164,6 +164,7 @@ static int adjm_run(ibfs_handle* h, int nsteps, int K, const double* wx, const d
                     double* dJdA, double* ms_fwd, double* ms_total) {
   if (h->cases.size() != 1 || !h->cases[0].dc.moving || h->precision != 0 || !h->cg)
     return set_error(IBFS_ERR_ARG, "the pitch adjoint needs a single pitching case (motion_kind 1) in the plain FP64 form");
+  if (h->cases[0].dc.nact) return set_error(IBFS_ERR_ARG, "the adjoint does not cover actuator jets");
   if (nsteps < 1 || K < 1 || !wx || !wy || !J || !dJdA) return set_error(IBFS_ERR_ARG, "bad adjoint arguments");
   HostCase& hc = h->cases[0];
   const DevCase& c = hc.dc;

@@ -417,6 +417,16 @@ static void build_step_program(ibfs_handle* h) {
     B.add([=]() { launch_move_body(dcases, d_mv, nmv, mnb, st); });
     B.add([=]() { launch_setup_reg_moving(dcases, d_mv, nmv, mnf, mpatch, st); });
   }
+  // actuator jets after the body motion (operators.f90:149-151)
+  std::vector<int> ac;
+  int mact = 0;
+  for (int i = 0; i < nc; i++)
+    if (cs[i].nact > 0) { ac.push_back(i); mact = std::max(mact, cs[i].nact); }
+  if (!ac.empty()) {
+    const int* d_ac = B.ints(ac);
+    int nac = (int)ac.size();
+    B.add([=]() { launch_actuate(dcases, d_ac, nac, mact, st); });
+  }
   // STEP 1 (operators.f90:97-134)
   std::vector<LevelItem> all;
   for (int i = 0; i < nc; i++) for (int k = 1; k <= cs[i].L; k++) all.push_back({i, k});
@@ -1220,6 +1230,38 @@ int ibfs_adjoint_run(ibfs_handle* h, int nsteps, int checkpoint_every, const dou
   int rc = adj_run(h, nsteps, checkpoint_every, body_vel, wx, wy, J, grad_vel, ms_forward, ms_total);
   if (rc) h->err = ibfs_last_error(nullptr);
   return rc;
+}
+
+int ibfs_set_actuators(ibfs_handle* h, int icase, int n_act, const int* npt, const double* u_j,
+                       const double* u_j_osc, const double* omg_j, const double* theta_j) {
+  if (!h) return IBFS_ERR_ARG;
+  if (icase < 0 || icase >= (int)h->cases.size() || n_act < 0 ||
+      (n_act > 0 && (!npt || !u_j || !u_j_osc || !omg_j || !theta_j)))
+    return fail(IBFS_ERR_ARG, "ibfs_set_actuators: bad arguments");
+  HostCase& c = h->cases[icase];
+  std::vector<double> tab;
+  const double pi = 3.1415926535897932384;
+  for (int a = 0; a < n_act; a++) {
+    if (npt[a] < 1) return fail(IBFS_ERR_ARG, "ibfs_set_actuators: an actuator needs at least one point");
+    for (int p = 0; p < npt[a]; p++) {
+      tab.push_back(u_j[a]);
+      tab.push_back(u_j_osc[a]);
+      tab.push_back(omg_j[a]);
+      tab.push_back(std::cos(pi / 180.0 * theta_j[a]));
+      tab.push_back(std::sin(pi / 180.0 * theta_j[a]));
+    }
+  }
+  const int nact = (int)tab.size() / 5;
+  if (nact > c.nb) return fail(IBFS_ERR_ARG, "ibfs_set_actuators: more actuator points than body points");
+  c.dc.nact = nact;
+  c.dc.act = nact ? dupload(h, tab) : nullptr;
+  if (nact && !c.dc.act) return fail(IBFS_ERR_NOMEM, "device allocation failed (actuators)");
+  IBFS_CUDA_CHECK(cudaMemcpy(h->d_cases + icase, &c.dc, sizeof(DevCase), cudaMemcpyHostToDevice));
+  build_step_program(h);
+  IBFS_CUDA_CHECK(cudaDeviceSynchronize());
+  capture_graph(h);
+  IBFS_CUDA_CHECK(cudaGetLastError());
+  return IBFS_OK;
 }
 
 int ibfs_adjoint_pitch_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* wx, const double* wy,

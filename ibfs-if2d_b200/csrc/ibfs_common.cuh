@@ -66,6 +66,11 @@ struct DevCase {
   double* twsum;                 // [Nf] sum of a force's weights
   double* tq;                    // [Nf][9] (q + q0) at the force's faces, or null (adjoint capture)
 
+  // actuator jets (actuation / u_jet, grid.f90:579-633): the last nact body
+  // points, [nact][5] = u_j, u_j_osc, omg_j, cos(pi/180 theta_j), sin(pi/180 theta_j)
+  int nact;
+  const double* act;
+
   // conjugate gradient (operators.f90:393-441) on the force system
   double *cg_r, *cg_d, *cg_q, *cg_q2;  // [Nf]
   double* cg_sc;                       // delta_new, delta_old, eps, alpha

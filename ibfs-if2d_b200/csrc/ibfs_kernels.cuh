@@ -76,6 +76,7 @@ void launch_step_begin(const DevCase* cases, int ncases, cudaStream_t st);
 
 // Moving body and CG (grid.f90:523-576, 142-230; operators.f90:393-441).
 void launch_move_body(const DevCase* cases, const int* cids, int ncases, int max_nb, cudaStream_t st);
+void launch_actuate(const DevCase* cases, const int* cids, int ncases, int max_nact, cudaStream_t st);
 void launch_setup_reg_moving(const DevCase* cases, const int* cids, int ncases, int max_nf, int max_patch,
                              cudaStream_t st);
 void launch_cg_start(const DevCase* cases, const int* cids, int ncases, cudaStream_t st);

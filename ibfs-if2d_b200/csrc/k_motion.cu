@@ -35,6 +35,22 @@ __global__ void k_move_body(const DevCase* __restrict__ cases, const int* __rest
   C.bvel[C.nb + k] = thd * (x - C.pivot_x);
 }
 
+// Actuator jets (actuation, grid.f90:579-605; u_jet, :608-633): point
+// nb - nact + p gets the velocity u_jet = (u_j + u_j_osc sin(omg_j dt itime))
+// times (cos, sin)(pi/180 theta_j) of its actuator, after move_body; rhsf
+// multiplies it by delta as the reference's motion does. The parameters are
+// read once instead of from input/actuator.NNN.inp every step.
+__global__ void k_actuate(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
+  const DevCase& C = cases[cids[blockIdx.y]];
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= C.nact) return;
+  const double* a = C.act + 5 * p;
+  int k = C.nb - C.nact + p;
+  double u = a[0] + a[1] * sin(a[2] * C.dt * (double)(*C.itime));
+  C.bvel[k] = u * a[3];
+  C.bvel[C.nb + k] = u * a[4];
+}
+
 // Per-force table: u faces at (dx(i-1)-ox, dx(j-1)-oy+dx/2), v faces at
 // (dx(i-1)-ox+dx/2, dx(j-1)-oy); candidates scanned j-major for ascending
 // face index.
@@ -192,6 +208,9 @@ __global__ void k_copy_vec(double* const* __restrict__ dst, const double* const*
 
 void launch_move_body(const DevCase* cases, const int* cids, int ncases, int max_nb, cudaStream_t st) {
   if (ncases) k_move_body<<<dim3((max_nb + 127) / 128, ncases), 128, 0, st>>>(cases, cids);
+}
+void launch_actuate(const DevCase* cases, const int* cids, int ncases, int max_nact, cudaStream_t st) {
+  if (ncases) k_actuate<<<dim3((max_nact + 127) / 128, ncases), 128, 0, st>>>(cases, cids);
 }
 void launch_setup_reg_moving(const DevCase* cases, const int* cids, int ncases, int max_nf, int max_patch,
                              cudaStream_t st) {

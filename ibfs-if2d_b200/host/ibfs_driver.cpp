@@ -18,7 +18,14 @@
 //   advance    ibfs_advance per step; every isave steps and at istop the
 //              restart record; force.dat / circ.dat / slip.dat every step
 //              (operators.f90:176-188, 549-699)
-// Actuator points (bodyno < 0, grid.f90:579-718) are not supported.
+//   actuators  input/actuator.NNN.inp (&READ_ACT_PARAMETERS) for NNN = 001..100:
+//              when geom.inp already holds actuator points (bodyno < 0) their
+//              counts come from input/slot.NNN.inp; otherwise each actuator's
+//              slot points are appended (actuator_slot, writing slot.dat and
+//              slot.NNN.inp) and geom.inp is rewritten (grid.f90:286-325,
+//              382-401); the jets (actuation, grid.f90:579-633) then run on
+//              the device through ibfs_set_actuators, the namelists read once
+//              instead of every step
 //
 //   ibfs_gpu [-C dir] [--dry-run | --post]
 // --dry-run reads and checks the inputs (and a restart record when
@@ -129,25 +136,88 @@ int main(int argc, char** argv) {
 
   // SETUP GEOMETRY (grid.f90:252-353)
   Geometry geo;
-  if (file_exists("input/geom.inp")) {
+  const double ds = p.len / (double)p.m;
+  const bool from_inp = file_exists("input/geom.inp");
+  bool from_spec = false;
+  if (from_inp) {
     if (!read_geometry("input/geom.inp", geo, msg)) return stop(msg, 2);
     logline("Reading geometry from geom.inp");
     if (!dry) std::printf("Reading geometry from geom.inp\n");
   } else if (file_exists("input/geom.spec")) {  // primitives -> geom.inp
     bool ok = false;
     std::string spec = file_text("input/geom.spec", ok);
-    if (!ok || !geometry_from_spec(spec, p.len / (double)p.m, geo, msg)) return stop("input/geom.spec: " + msg, 2);
-    if (!dry && !write_geometry("input/geom.inp", geo, msg)) return stop(msg, 2);
-    logline("Generated geometry from primitives (input/geom.spec) into geom.inp");
+    if (!ok || !geometry_from_spec(spec, ds, geo, msg)) return stop("input/geom.spec: " + msg, 2);
+    from_spec = true;
   } else {
     geo = default_geometry(p);
   }
-  for (const std::string& w : spacing_warnings(geo, p.len / (double)p.m)) {
+  // ACTUATORS (grid.f90:286-325, 382-394)
+  auto numbered = [](const char* fmt, int i) {
+    char b[64];
+    std::snprintf(b, sizeof b, fmt, i);
+    return std::string(b);
+  };
+  bool defined = false;
+  for (int b : geo.bodyno) defined = defined || b < 0;
+  std::vector<Actuator> acts;  // actuators 1..n_act in order, with their point counts
+  std::vector<int> act_npt;
+  auto read_act = [&](int i, Actuator& a) {
+    std::string an = numbered("input/actuator.%03d.inp", i);
+    bool ok = false;
+    std::string text = file_text(an, ok);
+    if (!ok || !parse_act_parameters(text, a, msg)) {
+      msg = an + ": " + msg;
+      return false;
+    }
+    return true;
+  };
+  if (!(from_inp && defined)) {  // append each actuator's slot points
+    for (int i = 1; i <= 100; i++) {
+      if (!file_exists(numbered("input/actuator.%03d.inp", i))) continue;
+      Actuator a;
+      if (!read_act(i, a)) return stop(msg, 2);
+      int np = actuator_slot(a.x_j, a.y_j, a.h_j, ds, a.theta_j, -i, geo, !dry, msg);
+      if (np < 0) return stop(msg, 2);
+      acts.push_back(a);
+      act_npt.push_back(np);
+    }
+  } else {  // points already in geom.inp: counts from slot.NNN.inp
+    int n = 0;
+    for (int i = 1; i <= 100; i++)
+      if (file_exists(numbered("input/actuator.%03d.inp", i))) n++;
+    for (int i = 1; i <= n; i++) {
+      Actuator a;
+      if (!read_act(i, a)) return stop(msg, 2);
+      std::string sn = numbered("input/slot.%03d.inp", i);
+      bool ok = false;
+      int np = 0;
+      std::string st = file_text(sn, ok);
+      if (!ok || std::sscanf(st.c_str(), "%d", &np) != 1 || np < 1)
+        return stop("cannot read the point count in " + sn, 2);
+      acts.push_back(a);
+      act_npt.push_back(np);
+    }
+  }
+  const int n_act = (int)acts.size();
+  int n_act_pt = 0;
+  for (int np : act_npt) n_act_pt += np;
+  if (n_act_pt > (int)geo.x.size()) return stop("the actuators have more points than the geometry", 2);
+  if (!dry && (!from_inp || (n_act > 0 && !defined))) {  // geometry written for the next run
+    if (!write_geometry("input/geom.inp", geo, msg)) return stop(msg, 2);
+    if (from_spec) logline("Generated geometry from primitives (input/geom.spec) into geom.inp");
+    if (n_act > 0) logline("...appended actuator info to geom.inp");
+  }
+  std::vector<double> act_u, act_osc, act_omg, act_theta;
+  for (const Actuator& a : acts) {
+    act_u.push_back(a.u_j);
+    act_osc.push_back(a.u_j_osc);
+    act_omg.push_back(a.omg_j);
+    act_theta.push_back(a.theta_j);
+  }
+  for (const std::string& w : spacing_warnings(geo, ds)) {
     std::fprintf(stderr, "%s\n", w.c_str());
     logline(w);
   }
-  for (int b : geo.bodyno)
-    if (b < 0) return stop("actuator points (bodyno < 0) are not supported by this driver", 2);
   const int nb = (int)geo.x.size();
 
   if (dry) {
@@ -172,12 +242,12 @@ int main(int argc, char** argv) {
                 "\"offsetx\": %.17g, \"offsety\": %.17g, \"mgridlev\": %d, \"make_vortex\": %d, "
                 "\"stationary\": %d, \"precision\": %d, \"cg_relative\": %d, \"motion_kind\": %d, "
                 "\"tile_cfg\": %d, \"nb\": %d, \"x0\": %.17g, \"y0\": %.17g, \"xsum\": %.17g, \"ysum\": %.17g, "
-                "\"var_sums\": [",
+                "\"n_act\": %d, \"n_act_pt\": %d, \"var_sums\": [",
                 p.istart, p.istop, p.isave, p.m, p.n, p.dt, p.re, p.cgtol, p.cg_max_iter, p.unif_flow, p.len,
                 p.offsetx, p.offsety, p.mgridlev, p.make_vortex, p.stationary, opt.precision, opt.cg_relative,
                 opt.motion_kind, opt.tile_cfg, nb, nb ? geo.x[0] : 0.0, nb ? geo.y[0] : 0.0,
                 [&] { double t = 0.0; for (double v : geo.x) t += v; return t; }(),
-                [&] { double t = 0.0; for (double v : geo.y) t += v; return t; }());
+                [&] { double t = 0.0; for (double v : geo.y) t += v; return t; }(), n_act, n_act_pt);
     for (size_t i = 0; i < var_sums.size(); i++) std::printf("%s%.17g", i ? ", " : "", var_sums[i]);
     std::printf("]}\n");
     return 0;
@@ -187,6 +257,11 @@ int main(int argc, char** argv) {
   ibfs_handle* h = nullptr;
   int rc = ibfs_create(&p, &opt, nb, geo.x.data(), geo.y.data(), geo.bodyno.data(), &h);
   if (rc) return stop(std::string("ibfs_create: ") + ibfs_last_error(h), 10 + rc);
+  if (n_act > 0) {
+    rc = ibfs_set_actuators(h, 0, n_act, act_npt.data(), act_u.data(), act_osc.data(), act_omg.data(),
+                            act_theta.data());
+    if (rc) return stop(std::string("ibfs_set_actuators: ") + ibfs_last_error(h), 10 + rc);
+  }
   int m, n, L, nq, nbb, nbody;
   ibfs_case_sizes(h, 0, &m, &n, &L, &nq, &nbb, &nbody);
   const size_t ns = (size_t)(m - 1) * (n - 1);

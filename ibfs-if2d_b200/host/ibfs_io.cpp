@@ -205,6 +205,30 @@ bool parse_b200_options(const std::string& text, ibfs_options_c& o, std::string&
   return true;
 }
 
+bool parse_act_parameters(const std::string& text, Actuator& a, std::string& msg) {
+  bool found = false;
+  std::string body = group_body(text, "READ_ACT_PARAMETERS", found);
+  if (!found) {
+    msg = "no &READ_ACT_PARAMETERS group";
+    return false;
+  }
+  std::vector<std::pair<std::string, std::string>> kv;
+  if (!pairs(body, kv, msg)) return false;
+  for (auto& [k, v] : kv) {
+    double* dst = k == "X_J" ? &a.x_j : k == "Y_J" ? &a.y_j : k == "H_J" ? &a.h_j : k == "U_J" ? &a.u_j
+                : k == "U_J_OSC" ? &a.u_j_osc : k == "THETA_J" ? &a.theta_j : k == "OMG_J" ? &a.omg_j : nullptr;
+    if (!dst) {
+      msg = "unknown namelist item " + k;
+      return false;
+    }
+    if (!to_double(v, *dst)) {
+      msg = "bad value '" + v + "' for " + k;
+      return false;
+    }
+  }
+  return true;
+}
+
 std::string format_read_parameters(const ibfs_params_c& p) {
   char b[1024];
   auto L = [](int v) { return v ? "T" : "F"; };
@@ -478,6 +502,50 @@ std::string real_item(double x) {
   return std::string(" ") + b;
 }
 }  // namespace
+
+int actuator_slot(double x, double y, double hs, double ds, double angle, int num, Geometry& g, bool write_files,
+                  std::string& msg) {
+  const double pi = 3.1415926535897932384;
+  const int npt = (int)(hs / ds);
+  if (npt == 0) {
+    g.x.push_back(x);
+    g.y.push_back(y);
+    g.bodyno.push_back(num);
+  } else {
+    const double a = pi * (angle + 90.0) / 180.0;
+    for (int i = 1; i <= npt + 1; i++) {
+      const double seg = (double)(float)(i - 1) * hs / (double)(float)npt;
+      g.x.push_back(x - hs / 2.0 * std::cos(a) + seg * std::cos(a));
+      g.y.push_back(y - hs / 2.0 * std::sin(a) + seg * std::sin(a));
+      g.bodyno.push_back(num);
+    }
+  }
+  if (!write_files) return npt + 1;
+  char name[64];
+  std::snprintf(name, sizeof name, "input/slot.%03d.inp", -num);
+  // slot.dat is replaced by the first actuator and appended to by the others;
+  // slot.NNN.inp is replaced by actuator 1, appended to otherwise (grid.f90:682-698)
+  FILE* f1 = std::fopen("input/slot.dat", num == -1 ? "w" : "a");
+  FILE* f2 = std::fopen(name, num == -1 ? "w" : "a");
+  if (!f1 || !f2) {
+    if (f1) std::fclose(f1);
+    if (f2) std::fclose(f2);
+    msg = std::string("cannot write input/slot.dat or ") + name;
+    return -1;
+  }
+  std::fprintf(f1, "  ----------- ACTUATOR No. %12d\n", -num);
+  std::fprintf(f1, "    o Desired slot width               = %s\n", real_item(hs).c_str());
+  std::fprintf(f1, "    o Actual slot width in simulation  = %s\n", real_item(npt == 0 ? ds : hs).c_str());
+  std::fprintf(f1, "    o Number of pts used to model slot = %12d\n", npt + 1);
+  std::fprintf(f2, "%12d\n", npt + 1);
+  bool ok = std::fclose(f1) == 0;
+  ok = std::fclose(f2) == 0 && ok;
+  if (!ok) {
+    msg = std::string("write failed: ") + name;
+    return -1;
+  }
+  return npt + 1;
+}
 
 std::string list_directed(int it, const std::vector<double>& v) {
   char b[32];

@@ -33,6 +33,14 @@ bool parse_read_parameters(const std::string& text, ibfs_params_c& p, std::strin
 // group; absent group = zero-initialised options (reference behaviour).
 bool parse_b200_options(const std::string& text, ibfs_options_c& o, std::string& msg);
 
+// &READ_ACT_PARAMETERS of input/actuator.NNN.inp (grid.f90:263-264, 616-623):
+// slot centre, width, jet speed, its oscillating part, angle (degrees) and
+// angular frequency; absent items stay zero.
+struct Actuator {
+  double x_j = 0.0, y_j = 0.0, h_j = 0.0, u_j = 0.0, u_j_osc = 0.0, theta_j = 0.0, omg_j = 0.0;
+};
+bool parse_act_parameters(const std::string& text, Actuator& a, std::string& msg);
+
 // The namelist written when input/ibfs.inp is absent (parameters.f90:64-66).
 std::string format_read_parameters(const ibfs_params_c& p);
 
@@ -56,6 +64,15 @@ Geometry default_geometry(const ibfs_params_c& p);
 // grid spacing len/m. Returns false with msg on a malformed line.
 bool geometry_from_spec(const std::string& text, double ds, Geometry& g, std::string& msg);
 bool write_geometry(const std::string& path, const Geometry& g, std::string& msg);
+
+// actuator_slot (grid.f90:636-718): appends to g the INT(hs/ds)+1 points of a
+// slot of width hs centred at (x, y) across the jet angle (degrees), spacing
+// hs/INT(hs/ds), or the single point (x, y) when INT(hs/ds) = 0, with body
+// number num (-actuator number). With write_files it also writes the user
+// summary input/slot.dat and the point count input/slot.NNN.inp as the
+// reference does. Returns the point count, or -1 with msg on a write failure.
+int actuator_slot(double x, double y, double hs, double ds, double angle, int num, Geometry& g, bool write_files,
+                  std::string& msg);
 
 // The check the reference leaves out (grid.f90:280-284): for every body, the
 // distance between consecutive points against ds; one message per body whose

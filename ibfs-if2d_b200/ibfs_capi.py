@@ -26,6 +26,7 @@ EXPORTS = [
     "ibfs_advance", "ibfs_advance_n", "ibfs_batch_advance", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
     "ibfs_last_cg_iterations", "ibfs_adjoint_run", "ibfs_adjoint_pitch_run", "ibfs_vertex_fields",
+    "ibfs_set_actuators",
     "ibfs_last_error",
 ]
 
@@ -93,6 +94,7 @@ def lib():
         L.ibfs_last_cg_iterations.argtypes = [vp]
         L.ibfs_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
         L.ibfs_adjoint_pitch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]
+        L.ibfs_set_actuators.argtypes = [vp, ctypes.c_int, ctypes.c_int, _IP, _DP, _DP, _DP, _DP]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
         L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
@@ -260,6 +262,16 @@ class Solver:
                                            ctypes.byref(J), _p(grad), ctypes.byref(ms_f), ctypes.byref(ms_t)))
         self.itime.value += nsteps
         return J.value, grad, ms_f.value, ms_t.value
+
+    def set_actuators(self, actuators, icase=0):
+        """Actuator jets on the last body points of case icase (see
+        ibfs_set_actuators): a list of dicts with npt, u_j, u_j_osc, omg_j,
+        theta_j, in actuator order; [] removes them."""
+        n = len(actuators)
+        npt = np.array([a["npt"] for a in actuators] or [0], dtype=np.int32)
+        col = {k: np.array([float(a[k]) for a in actuators] or [0.0]) for k in ("u_j", "u_j_osc", "omg_j", "theta_j")}
+        self._check(lib().ibfs_set_actuators(self.h, icase, n, npt.ctypes.data_as(_IP), _p(col["u_j"]),
+                                             _p(col["u_j_osc"]), _p(col["omg_j"]), _p(col["theta_j"])))
 
     def adjoint_pitch_run(self, nsteps, checkpoint_every, wx, wy):
         """J and dJ/d(pitch amplitude, per degree) over nsteps advances of a

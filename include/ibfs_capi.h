@@ -176,6 +176,20 @@ int ibfs_kernels_per_step(const ibfs_handle* h);
 int ibfs_adjoint_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* body_vel, const double* wx,
                      const double* wy, double* J, double* grad_vel, double* ms_forward, double* ms_total);
 
+/* Actuator jets (the reference's actuation, grid.f90:579-605, and u_jet,
+ * :608-633): the last sum(npt) body points of case icase, npt[a] points per
+ * actuator a = 0..n_act-1 in that order (the slot points actuator_slot
+ * appends, grid.f90:636-718), get every step the velocity
+ *   u_jet = (u_j + u_j_osc sin(omg_j dt itime)) (cos, sin)(pi/180 theta_j)
+ * (flow units, multiplied by delta in the force system like the motion
+ * vector), computed on the device after any body motion and overriding the
+ * body velocities passed to ibfs_advance for those points. The parameters are
+ * those of input/actuator.NNN.inp (&READ_ACT_PARAMETERS); the reference reads
+ * them from the file every step. n_act = 0 removes the jets. Rebuilds the step
+ * graph; call between advances. */
+int ibfs_set_actuators(ibfs_handle* h, int icase, int n_act, const int* npt, const double* u_j,
+                       const double* u_j_osc, const double* omg_j, const double* theta_j);
+
 /* Discrete adjoint of nsteps advances of a single rigidly pitching body (no
  * reference counterpart): motion_kind 1, stationary = .FALSE. (CG force
  * solve, cjgr operators.f90:393-441), plain FP64 form. From the current state

@@ -118,6 +118,39 @@ def line(ds, length, aoa, x=0.0, y=0.0, npt=None):
     return xb, yb
 
 
+def actuator_slot(x, y, hs, ds, angle, num):
+    """grid.f90:636-680: the points of one actuator slot of width hs centred at
+    (x, y) across the jet direction angle (degrees): INT(hs/ds)+1 points at
+    spacing hs/INT(hs/ds), or the single point (x, y) when INT(hs/ds) = 0;
+    body number num (negative). Returns xb, yb, bodyno."""
+    npt = int(hs / ds)
+    if npt == 0:
+        return np.array([x]), np.array([y]), np.array([num], dtype=np.int32)
+    a = PI * (angle + 90.0) / 180.0
+    seg = np.arange(npt + 1, dtype=np.float64) * hs / float(npt)
+    xb = x - hs / 2.0 * math.cos(a) + seg * math.cos(a)
+    yb = y - hs / 2.0 * math.sin(a) + seg * math.sin(a)
+    return xb, yb, np.full(npt + 1, num, dtype=np.int32)
+
+
+def jet_velocities(vel, actuators, itime, dt):
+    """actuation (grid.f90:579-605) with u_jet (:608-633): the last points of the
+    body-velocity vector vel (x components, then y), npt per actuator in
+    order, get (u_j + u_j_osc sin(omg_j dt itime)) (cos, sin)(pi/180 theta_j).
+    actuators: list of dicts npt, u_j, u_j_osc, omg_j, theta_j. Returns a copy."""
+    v = np.array(vel, dtype=np.float64)
+    nb = v.size // 2
+    k = nb - sum(a["npt"] for a in actuators)
+    for a in actuators:
+        u = a["u_j"] + a["u_j_osc"] * math.sin(a["omg_j"] * dt * float(itime))
+        cx, sy = math.cos(PI / 180.0 * a["theta_j"]), math.sin(PI / 180.0 * a["theta_j"])
+        for _ in range(a["npt"]):
+            v[k] = u * cx
+            v[nb + k] = u * sy
+            k += 1
+    return v
+
+
 class Case:
     """One oracle case (grid + state), mirroring the reference's globals."""
 

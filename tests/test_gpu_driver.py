@@ -113,3 +113,36 @@ def test_driver_run_restart_and_cholesky_file(tmp_path):
                     # plus the FP64 parity bar (1e-10 of the field) for values at roundoff level
                     bar = 5.01e-5 * np.abs(ref[f]) + 1e-10 * np.abs(ref[f]).max() + 1e-300
                     assert np.all(np.abs(data[:, 2 + c] - ref[f]) <= bar), (k, f)
+
+
+@pytest.mark.skipif(not os.path.exists(DRIVER), reason="driver not built")
+def test_driver_actuator_jets(tmp_path):
+    """input/actuator.001.inp: the driver appends the slot points to the
+    geometry (bodyno -1), writes slot.001.inp and rewrites geom.inp, and runs
+    the jets on the device; force.dat carries bodies -1 and 0 (write_force
+    loops minval..maxval of bdyno) and matches the oracle advanced with the
+    jet velocities computed on the host."""
+    import math
+    d = tmp_path / "act"
+    xb, yb = setup_dir(d)
+    a = dict(x_j=0.0, y_j=0.75, h_j=0.3, u_j=0.5, u_j_osc=0.2, theta_j=90.0, omg_j=2.0 * math.pi)
+    body = ", ".join(f"{k.upper()} = {v!r}" for k, v in a.items())
+    (d / "input" / "actuator.001.inp").write_text(f" &READ_ACT_PARAMETERS {body} /\n")
+    run(d)
+    ax, ay, ab = O.actuator_slot(a["x_j"], a["y_j"], a["h_j"], 4.0 / M, a["theta_j"], -1)
+    assert int(open(d / "input" / "slot.001.inp").read().split()[0]) == len(ax)
+    geo = open(d / "input" / "geom.inp").read().split()
+    assert int(geo[0]) == len(xb) + len(ax)
+    x, y = np.concatenate([xb, ax]), np.concatenate([yb, ay])
+    bd = np.concatenate([np.zeros(len(xb), dtype=np.int32), ab])
+    oc = O.Case(O.make_params(M, M, DT, RE, LEV), x, y, bd)
+    acts = [dict(npt=len(ax), u_j=a["u_j"], u_j_osc=a["u_j_osc"], omg_j=a["omg_j"], theta_j=a["theta_j"])]
+    ref = []
+    for s in range(1, STEPS + 1):
+        rc, o = oc.advance(body_vel=O.jet_velocities(np.zeros(2 * len(x)), acts, s, DT))
+        assert rc == 0
+        ref.append(list(o["fx"]) + list(o["fy"]))
+    ref = np.array(ref)
+    f = table(d / "output" / "force.dat")
+    assert f.shape == (STEPS, 5)
+    assert np.abs(f[:, 1:] - ref).max() <= 1e-10 * np.abs(ref).max()

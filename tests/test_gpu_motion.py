@@ -105,9 +105,10 @@ def test_pitching_batch_equals_single_handles():
 
 def test_amplitude_derivative_by_central_differences():
     """d(mean drag)/d(pitch amplitude) from one batch of A -+ h cases: the
-    central differences at two step sizes agree (O(h^2) truncation), and J (the
+    central differences at two step sizes agree (O(h^2) truncation), J (the
     mean of the two neighbours, O(h^2) from J(A)) is the mean drag of a
-    single-handle run at A within that."""
+    single-handle run at A within that, and the discrete adjoint agrees with
+    the extrapolated difference."""
     import sensitivity as S
     kw = dict(m=48, levels=2, re=500.0, dt=0.01, freq=0.25)
     amps = [10.0, 25.0]
@@ -122,3 +123,9 @@ def test_amplitude_derivative_by_central_differences():
     h = s.advance_n(12)
     J = np.mean([s.outputs_of(h[k], 0)["fx"][0] for k in range(6, 12)])
     assert abs(J2[0] - J) <= 1e-5 * abs(J)
+    # the discrete adjoint against the Richardson extrapolation of the two
+    # central differences (O(h^4))
+    Ja, ga = S.mean_drag_amplitude_adjoint(amps, steps=12, tail=6, checkpoint_every=4, **kw)
+    assert abs(Ja[0] - J) <= 1e-12 * abs(J)
+    gr = (4.0 * g2 - g1) / 3.0
+    assert np.all(np.abs(ga - gr) <= 1e-5 * np.abs(gr)), (ga, gr)

@@ -122,3 +122,46 @@ def test_geometry_primitives_and_spacing_check(tmp_path):
     (tmp_path / "input" / "geom.spec").write_text("ellipse 1 2 0\n")
     rc, out, err = run(tmp_path)
     assert rc != 0 and "unknown primitive" in err
+
+
+def test_actuator_slots(tmp_path):
+    """input/actuator.NNN.inp (&READ_ACT_PARAMETERS): the slot points are
+    appended to the geometry as the reference's actuator_slot makes them
+    (grid.f90:636-680, restated in the oracle), one point when the slot is
+    narrower than ds; with geom.inp already holding them (bodyno < 0) the
+    counts come from slot.NNN.inp (grid.f90:286-301)."""
+    import oracle as O
+    m = 48
+    ds = 4.0 / m
+    write_inp(tmp_path, f"&READ_PARAMETERS M = {m}, N = {m}, LEN = 4.0, OFFSETX = 2, OFFSETY = 2, "
+                        "STATIONARY = T /\n")
+    (tmp_path / "input" / "geom.inp").write_text("2\n 0.5 0.0 0\n -0.5 0.0 0\n")
+    acts = [dict(x_j=0.0, y_j=0.75, h_j=0.3, u_j=0.5, u_j_osc=0.2, theta_j=90.0, omg_j=6.283185307179586),
+            dict(x_j=0.1, y_j=-0.8, h_j=0.05, u_j=-0.3, u_j_osc=0.1, theta_j=-60.0, omg_j=3.0)]
+    for i, a in enumerate(acts):
+        body = ", ".join(f"{k.upper()} = {v!r}" for k, v in a.items())
+        (tmp_path / "input" / f"actuator.{i + 1:03d}.inp").write_text(f" &READ_ACT_PARAMETERS {body} /\n")
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    p = json.loads(out)
+    pts = [O.actuator_slot(a["x_j"], a["y_j"], a["h_j"], ds, a["theta_j"], -(i + 1)) for i, a in enumerate(acts)]
+    npt = [len(x) for x, _, _ in pts]
+    assert npt == [int(0.3 / ds) + 1, 1]
+    assert (p["n_act"], p["n_act_pt"], p["nb"]) == (2, sum(npt), 2 + sum(npt))
+    xs = 0.5 - 0.5 + sum(float(x.sum()) for x, _, _ in pts)
+    ys = sum(float(y.sum()) for _, y, _ in pts)
+    assert abs(p["xsum"] - xs) <= 1e-14 and abs(p["ysum"] - ys) <= 1e-14
+    # geometry with the actuator points already in it (a restart directory)
+    lines = [" 0.5 0.0 0", " -0.5 0.0 0"]
+    for x, y, b in pts:
+        lines += [f" {float(xv)!r} {float(yv)!r} {int(bv)}" for xv, yv, bv in zip(x, y, b)]
+    (tmp_path / "input" / "geom.inp").write_text(f"{len(lines)}\n" + "\n".join(lines) + "\n")
+    for i, n in enumerate(npt):
+        (tmp_path / "input" / f"slot.{i + 1:03d}.inp").write_text(f"{n:12d}\n")
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    p = json.loads(out)
+    assert (p["n_act"], p["n_act_pt"], p["nb"]) == (2, sum(npt), 2 + sum(npt))
+    (tmp_path / "input" / "slot.002.inp").unlink()
+    rc, out, err = run(tmp_path)
+    assert rc != 0 and "slot.002.inp" in err
