@@ -110,6 +110,16 @@ MODULE ibfs_gpu
        TYPE(C_PTR), VALUE :: hist
      END FUNCTION ibfs_advance_n
 
+     ! actuator jets on the last sum(npt) body points (actuation, grid.f90:579-633)
+     INTEGER(C_INT) FUNCTION ibfs_set_actuators(h, icase, n_act, npt, u_j, u_j_osc, omg_j, theta_j) &
+          BIND(C, name="ibfs_set_actuators")
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       TYPE(C_PTR), VALUE :: h
+       INTEGER(C_INT), VALUE :: icase, n_act
+       INTEGER(C_INT), INTENT(IN) :: npt(*)
+       REAL(C_DOUBLE), INTENT(IN) :: u_j(*), u_j_osc(*), omg_j(*), theta_j(*)
+     END FUNCTION ibfs_set_actuators
+
      TYPE(C_PTR) FUNCTION ibfs_last_error(h) BIND(C, name="ibfs_last_error")
        IMPORT :: C_PTR
        TYPE(C_PTR), VALUE :: h

@@ -43,6 +43,9 @@ PROGRAM main_gpu
   ALLOCATE( fx(MAX(gnbody,1)), fy(MAX(gnbody,1)), circ(glev) )
   rc = ibfs_set_state(h, 0_C_INT, omega, fb, rhs_old, q, q0)
   CALL ibfs_stop_on(rc, h)
+  ! ACTUATOR JETS (actuation, grid.f90:579-633): setup counted n_act; the jets
+  ! run on the device with each actuator's namelist read once
+  IF (n_act > 0) CALL set_jets(n_act)
   IF (istart > 0 .AND. stationary) THEN   ! factor read by setup_variables
      rc = ibfs_set_cholesky(h, 0_C_INT, cholmat, cholvec)
      CALL ibfs_stop_on(rc, h)
@@ -87,6 +90,31 @@ PROGRAM main_gpu
   WRITE(111,*) "Total run time: ",cputime," s"
 
 CONTAINS
+
+  SUBROUTINE set_jets(na)
+    ! the parameters u_jet reads (grid.f90:616-623) and the point counts
+    ! actuation reads (grid.f90:592-595), for actuators 1..na in order
+    INTEGER, INTENT(IN) :: na
+    INTEGER(C_INT) :: npt(na), rcj
+    REAL(C_DOUBLE) :: uj(na), uosc(na), omg(na), th(na)
+    REAL(KIND(0.D0)) :: x_j, y_j, h_j, u_j, u_j_osc, theta_j, omg_j
+    NAMELIST /read_act_parameters/ x_j, y_j, h_j, u_j, u_j_osc, theta_j, omg_j
+    CHARACTER(3) :: act_num
+    INTEGER :: i
+    DO i = 1, na
+       WRITE(act_num,"(I3.3)") i
+       x_j = 0.d0; y_j = 0.d0; h_j = 0.d0; u_j = 0.d0; u_j_osc = 0.d0; theta_j = 0.d0; omg_j = 0.d0
+       OPEN(unit=7, file="input/actuator."//act_num//".inp", form="formatted", status="old")
+       READ(unit=7, nml=read_act_parameters)
+       CLOSE(7)
+       OPEN(unit=7, file="input/slot."//act_num//".inp", form="formatted", status="old")
+       READ(7,*) npt(i)
+       CLOSE(7)
+       uj(i) = u_j; uosc(i) = u_j_osc; omg(i) = omg_j; th(i) = theta_j
+    END DO
+    rcj = ibfs_set_actuators(h, 0_C_INT, INT(na, C_INT), npt, uj, uosc, omg, th)
+    CALL ibfs_stop_on(rcj, h)
+  END SUBROUTINE set_jets
 
   SUBROUTINE append_history(fname, it, vals)
     ! write_force / write_circ / write_slip file handling (operators.f90:564-573)
