@@ -10,6 +10,8 @@
 // (BM/16)x(BN/16) micro-tile on a strided lattice (conflict-free shared loads),
 // double-buffered shared memory with register prefetch. Grouped: blockIdx.y
 // selects a GemmDesc, blockIdx.x a tile of it.
+#include <mutex>
+
 #include "ibfs_common.cuh"
 #include "ibfs_kernels.cuh"
 
@@ -182,16 +184,17 @@ static void set_attr() {
                        (int)smem_bytes<BM, BN, DUAL>());
 }
 
-// Raise the dynamic shared-memory limit of every instantiation (called once
-// per process, before any stream capture).
+// Raise the dynamic shared-memory limit of every instantiation (once per
+// process, before any stream capture; handles may be created from several
+// host threads).
 void gemm_f64_init() {
-  static bool done = false;
-  if (done) return;
-  set_attr<64, 64, true>(); set_attr<64, 64, false>();
-  set_attr<32, 32, true>(); set_attr<32, 32, false>();
-  set_attr<64, 32, true>(); set_attr<64, 32, false>();
-  set_attr<32, 64, true>(); set_attr<32, 64, false>();
-  done = true;
+  static std::once_flag once;
+  std::call_once(once, []() {
+    set_attr<64, 64, true>(); set_attr<64, 64, false>();
+    set_attr<32, 32, true>(); set_attr<32, 32, false>();
+    set_attr<64, 32, true>(); set_attr<64, 32, false>();
+    set_attr<32, 64, true>(); set_attr<32, 64, false>();
+  });
 }
 
 template <int BM, int BN, bool DUAL>

@@ -16,22 +16,35 @@ import ibfs_capi as C
 import workloads as W
 
 
-def mean_drag_amplitude_adjoint(amps_deg, steps=100, tail=None, checkpoint_every=50, **case_kw):
+def mean_drag_amplitude_adjoint(amps_deg, steps=100, tail=None, checkpoint_every=50, workers=1, **case_kw):
     """J(A) and dJ/dA (per degree) for each amplitude in amps_deg by the
-    discrete adjoint; case_kw as for workloads.pitching."""
+    discrete adjoint; case_kw as for workloads.pitching. With workers > 1 the
+    single-case adjoints run from that many host threads at once, each handle
+    on its own stream (the library releases no shared state between handles;
+    results are bit-identical to a sequential run)."""
     tail = steps if tail is None else int(tail)
     wx = np.zeros(steps)
     wx[steps - tail:] = 1.0 / tail
     wy = np.zeros(steps)
-    J, g = [], []
+    solvers = []
     for a in np.asarray(amps_deg, dtype=np.float64):
         params, bodies, opts = W.solver_args([W.pitching(amp_deg=float(a), **case_kw)], C)
-        s = C.Solver(params[0], bodies[0], opts[0])
-        j, d, _, _ = s.adjoint_pitch_run(steps, checkpoint_every, wx, wy)
-        s.close()
-        J.append(j)
-        g.append(d)
-    return np.array(J), np.array(g)
+        solvers.append(C.Solver(params[0], bodies[0], opts[0]))
+
+    def run(s):
+        return s.adjoint_pitch_run(steps, checkpoint_every, wx, wy)
+
+    try:
+        if workers > 1:
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(workers) as ex:
+                res = list(ex.map(run, solvers))
+        else:
+            res = [run(s) for s in solvers]
+    finally:
+        for s in solvers:
+            s.close()
+    return np.array([r[0] for r in res]), np.array([r[1] for r in res])
 
 
 def mean_drag_amplitude_derivative(amps_deg, h_deg=1e-3, steps=100, tail=None, **case_kw):
