@@ -24,18 +24,30 @@ struct AdjCase {
   const double* tq;  // [nf][9] (q1 + q0) at each force's faces in that step (moving body)
 };
 
-void adj_curlT(const DevCase* c, const AdjCase* a, const DevCase& h, int nlev, int use_q1, cudaStream_t st);
-void adj_v2f_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st);
-void adj_getbcT(const DevCase* c, const double* ring, double* dst, const DevCase& h, double fac, cudaStream_t st);
-void adj_coarsifyT(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st);
-void adj_force(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st);
-void adj_solve(const DevCase* c, const double* in, double* tmp, double* out, const DevCase& h, cudaStream_t st);
-void adj_rhsf(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st);
-void adj_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, int first, cudaStream_t st);
-void adjm_reg_in(const DevCase* c, const AdjCase* a, const double* x, const DevCase& h, cudaStream_t st);
-void adjm_regT_curl0(const DevCase* c, const AdjCase* a, double* out, const DevCase& h, cudaStream_t st);
-void adjm_position(const DevCase* c, const AdjCase* a, const double* zcg, const double* u, double* acc,
-                   cudaStream_t st);
-void adj_nonlinear(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st);
+// The slots of one adjoint program: slot i differentiates case cids[i] of the
+// handle's device case array dc with working set da[i]; the maxima size the
+// grids (max_perim: nodes on the get_bc box perimeter).
+struct AdjGroup {
+  int n = 0;
+  const int* cids = nullptr;
+  const DevCase* dc = nullptr;
+  const AdjCase* da = nullptr;
+  int max_ns = 0, max_nq = 0, max_nf = 0, max_ring = 0, max_L = 0, max_perim = 0;
+};
+
+enum { GETBC_SBC = 0, GETBC_OBC = 1, GETBC_LB = 2 };
+
+void adj_curlT(const AdjGroup& g, int nlev, int use_q1, cudaStream_t st);
+void adj_v2f_level(const AdjGroup& g, int k, cudaStream_t st);
+void adj_getbcT(const AdjGroup& g, int which, int k, double fac, cudaStream_t st);
+void adj_coarsifyT(const AdjGroup& g, int k, cudaStream_t st);
+void adj_force(const AdjGroup& g, cudaStream_t st);
+void adj_solve(const AdjGroup& g, cudaStream_t st);
+void adj_rhsf(const AdjGroup& g, cudaStream_t st);
+void adjm_reg_in(const AdjGroup& g, const double* const* xs, cudaStream_t st);
+void adjm_regT_curl0(const AdjGroup& g, double* const* outs, cudaStream_t st);
+void adjm_position(const AdjGroup& g, const AdjCase* acg, const double* const* us, double* accs, cudaStream_t st);
+void adj_level(const AdjGroup& g, int k, int first, cudaStream_t st);
+void adj_nonlinear(const AdjGroup& g, int k, cudaStream_t st);
 
 }  // namespace ibfs

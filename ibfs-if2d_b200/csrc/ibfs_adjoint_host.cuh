@@ -11,161 +11,223 @@
 //      run the adjoint step backwards through the segment.
 // The adjoint step is one fixed launch program (captured as a CUDA graph);
 // per step only the pointers to the stored forward state and the objective
-// weights change, uploaded into the device AdjCase before each replay.
+// weights change, uploaded into the device AdjCase array before each replay.
+//
+// The programs serve a group of slots (one case each, differentiated
+// together, as the pitching-body driver does for a batch): every stage is one
+// launch over all slots and the sine-transform GEMMs of all slots share one
+// grouped launch. Each per-slot buffer family is one contiguous block.
 
 namespace ibfs {
 
 struct AdjPlan {
-  AdjCase a{};
+  std::vector<int> cids;     // case of each slot
+  const int* d_cids = nullptr;
+  std::vector<AdjCase> a;    // per-slot working sets (host copy of d_a)
   AdjCase* d_a = nullptr;
-  AdjCase* h_a = nullptr;  // pinned staging of the per-step AdjCase, one slot per segment step
+  AdjGroup g;
+  double *blk_W = nullptr, *blk_W2 = nullptr, *blk_Lb = nullptr, *blk_P = nullptr, *blk_Q = nullptr,
+         *blk_Grad = nullptr, *blk_Rf = nullptr;
+  size_t n_W = 0, n_Lb = 0, n_Q = 0, n_F = 0;  // doubles in the node / ring / face / force blocks
+  AdjCase* h_a = nullptr;    // pinned staging of the per-step AdjCase arrays, [h_slots]
   int h_slots = 0;
   Prog bw, bw_first;
   cudaGraphExec_t g_bw = nullptr, g_bwf = nullptr;
   bool graphs = false;
-  size_t state = 0;  // doubles per stored state
+  std::vector<size_t> soff;  // offset of each slot's part of a stored state
+  size_t state = 0;          // doubles per stored state (all slots)
 };
 
-static void adj_add_ctci(ProgBuilder& B, const DevCase& c, const double* in, double* out, double* t1, double* t2) {
-  B.gemm({right_desc(c, in, t1)}, false);
-  B.gemm({left_desc(c, t1, t2, EPI_LAMINV, 1)}, false);
-  B.gemm({right_desc(c, t2, t1)}, false);
-  B.gemm({left_desc(c, t1, out, EPI_STORE, 1)}, false);
+static const DevCase& slot_case(ibfs_handle* h, const std::vector<int>& cids, int i) {
+  return h->cases[cids[i]].dc;
+}
+
+static AdjGroup make_group(ibfs_handle* h, const std::vector<int>& cids, const int* d_cids, const AdjCase* da) {
+  AdjGroup g;
+  g.n = (int)cids.size();
+  g.cids = d_cids;
+  g.dc = h->d_cases;
+  g.da = da;
+  for (int c : cids) {
+    const DevCase& d = h->cases[c].dc;
+    g.max_ns = std::max(g.max_ns, d.ns);
+    g.max_nq = std::max(g.max_nq, d.nq);
+    g.max_nf = std::max(g.max_nf, d.nf);
+    g.max_ring = std::max(g.max_ring, d.nring);
+    g.max_L = std::max(g.max_L, d.L);
+    g.max_perim = std::max(g.max_perim, 2 * (d.m / 2 + 1) + 2 * (d.n / 2 - 1));
+  }
+  return g;
+}
+
+// One contiguous block per buffer family; slot i's part starts after the
+// parts of slots < i. per(c) = doubles slot c needs.
+template <class F>
+static double* alloc_family(ibfs_handle* h, const std::vector<int>& cids, std::vector<AdjCase>& a,
+                            double* AdjCase::*field, F per, size_t* total = nullptr) {
+  size_t n = 0;
+  for (size_t i = 0; i < cids.size(); i++) n += per(slot_case(h, cids, (int)i));
+  double* blk = dalloc<double>(h, std::max<size_t>(n, 1));
+  if (!blk) return nullptr;
+  size_t o = 0;
+  for (size_t i = 0; i < cids.size(); i++) {
+    a[i].*field = blk + o;
+    o += per(slot_case(h, cids, (int)i));
+  }
+  if (total) *total = n;
+  return blk;
+}
+
+// One grouped GEMM launch over the slots whose level count reaches k;
+// make(i, case, descs) appends slot i's descriptors.
+template <class F>
+static void gemm_slots(ProgBuilder& B, ibfs_handle* h, const std::vector<int>& cids, int k, F make) {
+  std::vector<GemmDesc> ds;
+  for (int i = 0; i < (int)cids.size(); i++)
+    if (slot_case(h, cids, i).L >= k) make(i, slot_case(h, cids, i), ds);
+  B.gemm(ds, false);
+}
+
+// aZ1 = ainv(aW_1) of every slot (ainv, myfft.f90:112-124, is symmetric).
+static void adj_add_ainv(ProgBuilder& B, ibfs_handle* h, const std::vector<int>& cids, const std::vector<AdjCase>& a) {
+  using V = std::vector<GemmDesc>;
+  gemm_slots(B, h, cids, 1, [&](int i, const DevCase& c, V& d) { d.push_back(right_desc(c, a[i].aW, a[i].aT1)); });
+  gemm_slots(B, h, cids, 1, [&](int i, const DevCase& c, V& d) { d.push_back(left_desc(c, a[i].aT1, a[i].aT2, EPI_AINV, 1)); });
+  gemm_slots(B, h, cids, 1, [&](int i, const DevCase& c, V& d) { d.push_back(right_desc(c, a[i].aT2, a[i].aT1)); });
+  gemm_slots(B, h, cids, 1, [&](int i, const DevCase& c, V& d) { d.push_back(left_desc(c, a[i].aT1, a[i].aZ1, EPI_STORE, 1)); });
 }
 
 // Adjoint of vort2flux(vel, omega, nlev) (operators.f90:191-240): incoming
 // adjoints of the fluxes (aQ, or aQ1 for nlev = 1) and of the coarsified
 // omega (aW); aW becomes the adjoint of the omega passed in.
-static void adj_add_v2f(ProgBuilder& B, const DevCase* dc, const AdjCase* da, const DevCase& c, const AdjCase& a,
-                        int nlev, int use_q1) {
-  cudaStream_t st = B.h->st;
-  DevCase hc = c;
-  B.add([=]() { adj_curlT(dc, da, hc, nlev, use_q1, st); });
-  for (int k = 1; k <= c.L; k++) {
-    adj_add_ctci(B, c, a.aS + (size_t)(k - 1) * c.ns, a.aZ1, a.aT1, a.aT2);
-    B.add([=]() { adj_v2f_level(dc, da, hc, k, st); });
-    if (k < c.L) {
-      const double* ring = a.aSbc + (size_t)(k - 1) * c.nring;
-      double* dst = a.aS + (size_t)k * c.ns;
-      B.add([=]() { adj_getbcT(dc, ring, dst, hc, 1.0, st); });
-    }
+static void adj_add_v2f(ProgBuilder& B, ibfs_handle* h, const std::vector<int>& cids, const std::vector<AdjCase>& a,
+                        const AdjGroup& g, int nlev, int use_q1) {
+  using V = std::vector<GemmDesc>;
+  cudaStream_t st = h->st;
+  B.add([=]() { adj_curlT(g, nlev, use_q1, st); });
+  for (int k = 1; k <= g.max_L; k++) {
+    // aZ1 = ctci(aS_k)
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) { d.push_back(right_desc(c, a[i].aS + (size_t)(k - 1) * c.ns, a[i].aT1)); });
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) { d.push_back(left_desc(c, a[i].aT1, a[i].aT2, EPI_LAMINV, 1)); });
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) { d.push_back(right_desc(c, a[i].aT2, a[i].aT1)); });
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) { d.push_back(left_desc(c, a[i].aT1, a[i].aZ1, EPI_STORE, 1)); });
+    B.add([=]() { adj_v2f_level(g, k, st); });
+    if (k < g.max_L) B.add([=]() { adj_getbcT(g, GETBC_SBC, k, 1.0, st); });
   }
-  for (int k = c.L; k >= 2; k--) B.add([=]() { adj_coarsifyT(dc, da, hc, k, st); });
+  for (int k = g.max_L; k >= 2; k--) B.add([=]() { adj_coarsifyT(g, k, st); });
 }
 
 // Adjoint step, first part: steps (7) and (6) of the forward step run
 // backwards, ending with the adjoint of fb (aF).
 static void adj_build_head(ibfs_handle* h, AdjPlan& P, ProgBuilder& B) {
-  const DevCase& c = h->cases[0].dc;
-  const DevCase* dc = h->d_cases;
-  const AdjCase& a = P.a;
-  const AdjCase* da = P.d_a;
   cudaStream_t st = h->st;
-  DevCase hc = c;
-  double* aLb = a.aLb;
-  size_t lbb = sizeof(double) * c.L * c.nring;
-  B.add([=]() { cudaMemsetAsync(aLb, 0, lbb, st); });
+  const AdjGroup g = P.g;
+  double* lb = P.blk_Lb;
+  size_t lbb = sizeof(double) * P.n_Lb;
+  B.add([=]() { cudaMemsetAsync(lb, 0, lbb, st); });
   // (7) vort2flux(q, omega, L), operators.f90:177
-  adj_add_v2f(B, dc, da, c, a, c.L, 0);
+  adj_add_v2f(B, h, P.cids, P.a, g, g.max_L, 0);
   // (6) omega_1 -= ainv(rot(reg(fb))), operators.f90:174
-  B.gemm({right_desc(c, a.aW, a.aT1)}, false);
-  B.gemm({left_desc(c, a.aT1, a.aT2, EPI_AINV, 1)}, false);
-  B.gemm({right_desc(c, a.aT2, a.aT1)}, false);
-  B.gemm({left_desc(c, a.aT1, a.aZ1, EPI_STORE, 1)}, false);
-  B.add([=]() { adj_force(dc, da, hc, st); });
+  adj_add_ainv(B, h, P.cids, P.a);
+  B.add([=]() { adj_force(g, st); });
 }
 
 // Adjoint step, last part: from the adjoint of rhsf (aRf) through steps (4)
 // to (1).
 static void adj_build_tail(ibfs_handle* h, AdjPlan& P, ProgBuilder& B, int first) {
-  const DevCase& c = h->cases[0].dc;
-  const DevCase* dc = h->d_cases;
-  const AdjCase& a = P.a;
-  const AdjCase* da = P.d_a;
+  using V = std::vector<GemmDesc>;
   cudaStream_t st = h->st;
-  DevCase hc = c;
-  size_t nsL = (size_t)c.L * c.ns;
+  const AdjGroup g = P.g;
+  const std::vector<int>& cids = P.cids;
+  const std::vector<AdjCase>& a = P.a;
   // (4) rhsf = regT(q_1) - motion
-  B.add([=]() { adj_rhsf(dc, da, hc, st); });
+  B.add([=]() { adj_rhsf(g, st); });
   // (3) vort2flux(q(:,1), omega, 1), operators.f90:163
-  adj_add_v2f(B, dc, da, c, a, 1, 1);
+  adj_add_v2f(B, h, cids, a, g, 1, 1);
   // (2) level loop k = L..1 run backwards (operators.f90:103-134)
-  double* aW2 = a.aW2;
-  B.add([=]() { cudaMemsetAsync(aW2, 0, sizeof(double) * nsL, st); });
-  for (int k = 1; k <= c.L; k++) {
-    double* Wk = a.aW + (size_t)(k - 1) * c.ns;
-    B.gemm({right_desc(c, Wk, a.aT1)}, false);
-    GemmDesc dd = left_desc(c, a.aT1, a.aZ1, EPI_ADJ_CN, k);
-    dd.C2 = a.aZ2;
-    B.gemm({dd}, false);
-    B.gemm({right_desc(c, a.aZ1, a.aT1), right_desc(c, a.aZ2, a.aT2)}, false);
-    B.gemm({left_desc(c, a.aT1, a.aA, EPI_STORE, k), left_desc(c, a.aT2, a.aW2 + (size_t)(k - 1) * c.ns, EPI_ADD, k)},
-           false);
-    B.add([=]() { adj_level(dc, da, hc, k, first, st); });
-    if (k < c.L) {
-      const double* ob = a.aObc;
-      double* dst = a.aW + (size_t)k * c.ns;
-      B.add([=]() { adj_getbcT(dc, ob, dst, hc, 0.25, st); });
-    }
-    B.add([=]() { adj_nonlinear(dc, da, hc, k, st); });
+  double* w2 = P.blk_W2;
+  size_t wb = sizeof(double) * P.n_W;
+  B.add([=]() { cudaMemsetAsync(w2, 0, wb, st); });
+  for (int k = 1; k <= g.max_L; k++) {
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) { d.push_back(right_desc(c, a[i].aW + (size_t)(k - 1) * c.ns, a[i].aT1)); });
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) {
+      GemmDesc dd = left_desc(c, a[i].aT1, a[i].aZ1, EPI_ADJ_CN, k);
+      dd.C2 = a[i].aZ2;
+      d.push_back(dd);
+    });
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) {
+      d.push_back(right_desc(c, a[i].aZ1, a[i].aT1));
+      d.push_back(right_desc(c, a[i].aZ2, a[i].aT2));
+    });
+    gemm_slots(B, h, cids, k, [&](int i, const DevCase& c, V& d) {
+      d.push_back(left_desc(c, a[i].aT1, a[i].aA, EPI_STORE, k));
+      d.push_back(left_desc(c, a[i].aT2, a[i].aW2 + (size_t)(k - 1) * c.ns, EPI_ADD, k));
+    });
+    B.add([=]() { adj_level(g, k, first, st); });
+    if (k < g.max_L) B.add([=]() { adj_getbcT(g, GETBC_OBC, k, 0.25, st); });
+    B.add([=]() { adj_nonlinear(g, k, st); });
   }
   // (1) lastbc(:,k) = get_bc(omega(:,:,k+1), 0.25), operators.f90:97-99
-  for (int k = 1; k < c.L; k++) {
-    const double* ring = a.aLb + (size_t)(k - 1) * c.nring;
-    double* dst = a.aW2 + (size_t)k * c.ns;
-    B.add([=]() { adj_getbcT(dc, ring, dst, hc, 0.25, st); });
-  }
-  double* aW = a.aW;
-  B.add([=]() { cudaMemcpyAsync(aW, aW2, sizeof(double) * nsL, cudaMemcpyDeviceToDevice, st); });
+  for (int k = 1; k < g.max_L; k++) B.add([=]() { adj_getbcT(g, GETBC_LB, k, 0.25, st); });
+  double* w = P.blk_W;
+  B.add([=]() { cudaMemcpyAsync(w, w2, wb, cudaMemcpyDeviceToDevice, st); });
 }
 
 // The whole adjoint step of a stationary body: (5) fb = cholsl(rhsf) is
 // symmetric, so its adjoint is the same two triangular solves.
 static void adj_build(ibfs_handle* h, AdjPlan& P, Prog& prog, int first) {
-  const DevCase& c = h->cases[0].dc;
-  const DevCase* dc = h->d_cases;
-  const AdjCase& a = P.a;
-  cudaStream_t st = h->st;
   ProgBuilder B{h, prog};
-  DevCase hc = c;
+  const AdjGroup g = P.g;
+  cudaStream_t st = h->st;
   adj_build_head(h, P, B);
-  double *aF = a.aF, *aTmp = a.aTmp, *aRf = a.aRf;
-  B.add([=]() { adj_solve(dc, aF, aTmp, aRf, hc, st); }, TAG_CHOL);
+  B.add([=]() { adj_solve(g, st); }, TAG_CHOL);
   adj_build_tail(h, P, B, first);
 }
 
-// Buffers of the adjoint working set of the handle's single case.
-static int adj_alloc(ibfs_handle* h, AdjPlan& P) {
-  const DevCase& c = h->cases[0].dc;
-  size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
-  AdjCase& a = P.a;
-  a.aW = dalloc<double>(h, nsL);
-  a.aW2 = dalloc<double>(h, nsL);
-  a.aP = dalloc<double>(h, nsL);
-  a.aQ = dalloc<double>(h, nqL);
-  a.aQ1 = dalloc<double>(h, c.nq);
-  a.aS = dalloc<double>(h, nsL);
-  a.aSbc = dalloc<double>(h, (size_t)c.L * c.nring);
-  a.aLb = dalloc<double>(h, (size_t)c.L * c.nring);
-  a.aObc = dalloc<double>(h, c.nring);
-  a.aA = dalloc<double>(h, c.ns);
-  a.aZ1 = dalloc<double>(h, c.ns);
-  a.aZ2 = dalloc<double>(h, c.ns);
-  a.aR = dalloc<double>(h, c.ns);
-  a.aT1 = dalloc<double>(h, c.ns);
-  a.aT2 = dalloc<double>(h, c.ns);
-  a.aF = dalloc<double>(h, c.nf);
-  a.aRf = dalloc<double>(h, c.nf);
-  a.aTmp = dalloc<double>(h, c.nf);
-  a.aGrad = dalloc<double>(h, c.nf);
-  P.d_a = dalloc<AdjCase>(h, 1);
-  if (!a.aW || !a.aQ || !a.aS || !a.aGrad || !P.d_a) return set_error(IBFS_ERR_NOMEM, "adjoint allocation failed");
-  P.state = 2 * nsL + nqL + c.nf;
+// Working sets of the slots (cases cids of the handle).
+static int adj_alloc(ibfs_handle* h, AdjPlan& P, const std::vector<int>& cids) {
+  P.cids = cids;
+  const int n = (int)cids.size();
+  P.a.assign(n, AdjCase{});
+  auto ns = [](const DevCase& c) { return (size_t)c.ns; };
+  auto nsL = [](const DevCase& c) { return (size_t)c.L * c.ns; };
+  auto nqL = [](const DevCase& c) { return (size_t)c.L * c.nq; };
+  auto nq = [](const DevCase& c) { return (size_t)c.nq; };
+  auto ringL = [](const DevCase& c) { return (size_t)c.L * c.nring; };
+  auto ring = [](const DevCase& c) { return (size_t)c.nring; };
+  auto nf = [](const DevCase& c) { return (size_t)c.nf; };
+  bool ok = true;
+  ok = ok && (P.blk_W = alloc_family(h, cids, P.a, &AdjCase::aW, nsL, &P.n_W));
+  ok = ok && (P.blk_W2 = alloc_family(h, cids, P.a, &AdjCase::aW2, nsL));
+  ok = ok && (P.blk_P = alloc_family(h, cids, P.a, &AdjCase::aP, nsL));
+  ok = ok && (P.blk_Q = alloc_family(h, cids, P.a, &AdjCase::aQ, nqL, &P.n_Q));
+  ok = ok && alloc_family(h, cids, P.a, &AdjCase::aQ1, nq);
+  ok = ok && alloc_family(h, cids, P.a, &AdjCase::aS, nsL);
+  ok = ok && alloc_family(h, cids, P.a, &AdjCase::aSbc, ringL);
+  ok = ok && (P.blk_Lb = alloc_family(h, cids, P.a, &AdjCase::aLb, ringL, &P.n_Lb));
+  ok = ok && alloc_family(h, cids, P.a, &AdjCase::aObc, ring);
+  for (double* AdjCase::*f : {&AdjCase::aA, &AdjCase::aZ1, &AdjCase::aZ2, &AdjCase::aR, &AdjCase::aT1, &AdjCase::aT2})
+    ok = ok && alloc_family(h, cids, P.a, f, ns);
+  ok = ok && alloc_family(h, cids, P.a, &AdjCase::aF, nf, &P.n_F);
+  ok = ok && (P.blk_Rf = alloc_family(h, cids, P.a, &AdjCase::aRf, nf));
+  ok = ok && alloc_family(h, cids, P.a, &AdjCase::aTmp, nf);
+  ok = ok && (P.blk_Grad = alloc_family(h, cids, P.a, &AdjCase::aGrad, nf));
+  P.d_a = dupload(h, P.a);
+  P.d_cids = dupload(h, cids);
+  if (!ok || !P.d_a || !P.d_cids) return set_error(IBFS_ERR_NOMEM, "adjoint allocation failed");
+  P.g = make_group(h, cids, P.d_cids, P.d_a);
+  P.soff.clear();
+  P.state = 0;
+  for (int i = 0; i < n; i++) {
+    const DevCase& c = slot_case(h, cids, i);
+    P.soff.push_back(P.state);
+    P.state += 2 * nsL(c) + nqL(c) + c.nf;
+  }
   return IBFS_OK;
 }
 
 static int adj_init(ibfs_handle* h, AdjPlan& P) {
-  int rc = adj_alloc(h, P);
+  int rc = adj_alloc(h, P, {0});
   if (rc) return rc;
   adj_build(h, P, P.bw, 0);
   adj_build(h, P, P.bw_first, 1);
@@ -174,22 +236,40 @@ static int adj_init(ibfs_handle* h, AdjPlan& P) {
   return IBFS_OK;
 }
 
-// state slot <-> case state (omega, rhs_old, q, fb)
-static void adj_save(ibfs_handle* h, double* slot) {
-  const DevCase& c = h->cases[0].dc;
-  size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
-  cudaMemcpyAsync(slot, c.omega, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
-  cudaMemcpyAsync(slot + nsL, c.rhs_old, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
-  cudaMemcpyAsync(slot + 2 * nsL, c.q, nqL * 8, cudaMemcpyDeviceToDevice, h->st);
-  cudaMemcpyAsync(slot + 2 * nsL + nqL, c.fb, (size_t)c.nf * 8, cudaMemcpyDeviceToDevice, h->st);
+// pinned staging for K per-step AdjCase arrays of the plan's slots
+static int adj_staging(AdjPlan& P, int K) {
+  int need = K * (int)P.cids.size();
+  if (P.h_slots >= need) return IBFS_OK;
+  if (P.h_a) cudaFreeHost(P.h_a);
+  P.h_a = nullptr;
+  P.h_slots = 0;
+  if (cudaMallocHost(&P.h_a, sizeof(AdjCase) * need) != cudaSuccess) return set_error(IBFS_ERR_NOMEM, "pinned allocation");
+  P.h_slots = need;
+  return IBFS_OK;
 }
-static void adj_restore(ibfs_handle* h, const double* slot) {
-  const DevCase& c = h->cases[0].dc;
-  size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
-  cudaMemcpyAsync(c.omega, slot, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
-  cudaMemcpyAsync(c.rhs_old, slot + nsL, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
-  cudaMemcpyAsync(c.q, slot + 2 * nsL, nqL * 8, cudaMemcpyDeviceToDevice, h->st);
-  cudaMemcpyAsync(c.fb, slot + 2 * nsL + nqL, (size_t)c.nf * 8, cudaMemcpyDeviceToDevice, h->st);
+
+// stored state <-> the slots' case states (omega, rhs_old, q, fb)
+static void adj_save(ibfs_handle* h, const AdjPlan& P, double* slot) {
+  for (size_t i = 0; i < P.cids.size(); i++) {
+    const DevCase& c = slot_case(h, P.cids, (int)i);
+    size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
+    double* s = slot + P.soff[i];
+    cudaMemcpyAsync(s, c.omega, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(s + nsL, c.rhs_old, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(s + 2 * nsL, c.q, nqL * 8, cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(s + 2 * nsL + nqL, c.fb, (size_t)c.nf * 8, cudaMemcpyDeviceToDevice, h->st);
+  }
+}
+static void adj_restore(ibfs_handle* h, const AdjPlan& P, const double* slot) {
+  for (size_t i = 0; i < P.cids.size(); i++) {
+    const DevCase& c = slot_case(h, P.cids, (int)i);
+    size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
+    const double* s = slot + P.soff[i];
+    cudaMemcpyAsync(c.omega, s, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(c.rhs_old, s + nsL, nsL * 8, cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(c.q, s + 2 * nsL, nqL * 8, cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(c.fb, s + 2 * nsL + nqL, (size_t)c.nf * 8, cudaMemcpyDeviceToDevice, h->st);
+  }
 }
 
 static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, const double* wx, const double* wy,
@@ -208,12 +288,7 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
     if (rc) return rc;
   }
   AdjPlan& P = *h->adj;
-  if (P.h_slots < K) {
-    if (P.h_a) cudaFreeHost(P.h_a);
-    P.h_a = nullptr;
-    if (cudaMallocHost(&P.h_a, sizeof(AdjCase) * K) != cudaSuccess) return set_error(IBFS_ERR_NOMEM, "pinned allocation");
-    P.h_slots = K;
-  }
+  if ((rc = adj_staging(P, K))) return rc;
   int nb = c.nbody;
   int nck = (nsteps + K - 1) / K;
   double *ck = nullptr, *seg = nullptr, *fin = nullptr, *w = nullptr, *hist = nullptr;
@@ -247,14 +322,14 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
   // 1. forward pass with checkpoints
   for (int s = 0; s < nsteps && rc == IBFS_OK; s++) {
     if (s % K == 0) {
-      adj_save(h, ck + P.state * (s / K));
+      adj_save(h, P, ck + P.state * (s / K));
       cudaMemcpyAsync(ck_it + s / K, c.itime, sizeof(int), cudaMemcpyDeviceToDevice, h->st);
     }
     rc = run_step(h);
     cudaMemcpyAsync(hist + (size_t)s * h->out_stride, h->d_out, sizeof(double) * h->out_stride,
                     cudaMemcpyDeviceToDevice, h->st);
   }
-  adj_save(h, fin);
+  adj_save(h, P, fin);
   cudaMemcpyAsync(ck_it + nck, c.itime, sizeof(int), cudaMemcpyDeviceToDevice, h->st);
   cudaEventRecord(e1, h->st);
   std::vector<double> hh((size_t)h->out_stride * nsteps);
@@ -267,12 +342,12 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
             wy[(size_t)s * nb + b] * hh[(size_t)s * h->out_stride + nb + b];
   *J = jj;
   // 2. backward pass
-  const AdjCase& a = P.a;
-  size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
-  cudaMemsetAsync(a.aW, 0, nsL * 8, h->st);
-  cudaMemsetAsync(a.aP, 0, nsL * 8, h->st);
-  cudaMemsetAsync(a.aQ, 0, nqL * 8, h->st);
-  cudaMemsetAsync(a.aGrad, 0, (size_t)c.nf * 8, h->st);
+  const AdjCase& a = P.a[0];
+  size_t nsL = (size_t)c.L * c.ns;
+  cudaMemsetAsync(P.blk_W, 0, P.n_W * 8, h->st);
+  cudaMemsetAsync(P.blk_P, 0, P.n_W * 8, h->st);
+  cudaMemsetAsync(P.blk_Q, 0, P.n_Q * 8, h->st);
+  cudaMemsetAsync(P.blk_Grad, 0, P.n_F * 8, h->st);
   for (int sg = nck - 1; sg >= 0 && rc == IBFS_OK; sg--) {
     int s0 = sg * K, s1 = std::min(nsteps, s0 + K);
     cudaStreamSynchronize(h->st);  // the pinned slots of the previous segment are free
@@ -280,11 +355,11 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
     // itself and the last step's result is not needed
     cudaMemcpyAsync(seg, ck + P.state * sg, sizeof(double) * P.state, cudaMemcpyDeviceToDevice, h->st);
     if (s1 - s0 > 1) {
-      adj_restore(h, ck + P.state * sg);
+      adj_restore(h, P, ck + P.state * sg);
       cudaMemcpyAsync(c.itime, ck_it + sg, sizeof(int), cudaMemcpyDeviceToDevice, h->st);
       for (int s = s0; s < s1 - 1 && rc == IBFS_OK; s++) {
         rc = run_step(h);
-        adj_save(h, seg + P.state * (s + 1 - s0));
+        adj_save(h, P, seg + P.state * (s + 1 - s0));
       }
     }
     for (int s = s1 - 1; s >= s0 && rc == IBFS_OK; s--) {
@@ -303,7 +378,7 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
       rc = run_prog(h, prog, P.graphs ? ex : nullptr);
     }
   }
-  adj_restore(h, fin);
+  adj_restore(h, P, fin);
   cudaMemcpyAsync(c.itime, ck_it + nck, sizeof(int), cudaMemcpyDeviceToDevice, h->st);
   cudaEventRecord(e2, h->st);
   cudaMemcpyAsync(grad, a.aGrad, sizeof(double) * c.nf, cudaMemcpyDeviceToHost, h->st);

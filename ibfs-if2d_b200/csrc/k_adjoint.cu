@@ -13,6 +13,10 @@
 // The DST-based inverses (ctci, ainv, the CN update) are symmetric and reuse
 // the forward sine-transform GEMMs; the Cholesky solve is symmetric too.
 // All kernels are gathers (no atomics), so the adjoint is deterministic.
+//
+// Every kernel serves a group of slots (cases differentiated together): slot
+// blockIdx.z is case cids[slot] with working set adj[slot]; grids are sized by
+// the group's largest case and a slot skips levels beyond its own L.
 #include "ibfs_adjoint.cuh"
 
 namespace ibfs {
@@ -22,11 +26,13 @@ __device__ __forceinline__ int ring_off(int m, int n, int side) {
 }
 
 // (s_hat, sbc_hat) = curl^T(q_hat) on level k; zero when k > nlev.
-__global__ void k_adj_curlT(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int nlev,
+__global__ void k_adj_curlT(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids, int nlev,
                             int use_q1) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
   int k = blockIdx.y + 1;
+  if (k > C.L) return;
   int m = C.m, n = C.n;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const double* Q = use_q1 ? A.aQ1 : A.aQ + (size_t)(k - 1) * C.nq;
@@ -107,9 +113,11 @@ __device__ __forceinline__ double getbcT_at(const double* __restrict__ ring, int
 }
 
 // aW_k += v ; sbc_hat_k += apply_bc^T(v) (vort2flux adjoint, one level).
-__global__ void k_adj_v2f_level(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adj_v2f_level(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids, int k) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  if (k > C.L) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const double* v = A.aZ1;
   if (t < C.ns) {
@@ -120,10 +128,20 @@ __global__ void k_adj_v2f_level(const DevCase* __restrict__ cases, const AdjCase
   }
 }
 
-// dst(a, b) += fac * get_bc^T(ring) on the box perimeter of a node field.
-__global__ void k_adj_getbcT(const DevCase* __restrict__ cases, const double* __restrict__ ring, double* dst,
-                             double fac) {
-  const DevCase& C = cases[0];
+// dst(a, b) += fac * get_bc^T(ring) on the box perimeter of a node field, for
+// the three uses of the adjoint (level k < L of the slot):
+//   GETBC_SBC  ring aSbc_k -> aS_{k+1}  (vort2flux, fac 1)
+//   GETBC_OBC  ring aObc   -> aW_{k+1}  (omega_bc of the CN update, fac 0.25)
+//   GETBC_LB   ring aLb_k  -> aW2_{k+1} (lastbc, fac 0.25)
+__global__ void k_adj_getbcT(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
+                             const int* __restrict__ cids, int which, int k, double fac) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  if (k >= C.L) return;
+  const double* ring = which == GETBC_SBC ? A.aSbc + (size_t)(k - 1) * C.nring
+                     : which == GETBC_OBC ? A.aObc : A.aLb + (size_t)(k - 1) * C.nring;
+  double* dst = (which == GETBC_SBC ? A.aS : which == GETBC_OBC ? A.aW : A.aW2) + (size_t)k * C.ns;
   int m = C.m, n = C.n;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   // perimeter nodes of the box [m/4,3m/4] x [n/4,3n/4]: bottom/top rows, then left/right columns
@@ -141,9 +159,11 @@ __global__ void k_adj_getbcT(const DevCase* __restrict__ cases, const double* __
 // coarsify^T (operators.f90:320-332): fine level k-1 gathers the coarse
 // centre of level k with the full-weighting weights; then the centre of
 // level k is cleared (it was overwritten in the forward pass).
-__global__ void k_adj_coarsifyT(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adj_coarsifyT(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids, int k) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  if (k > C.L) return;
   int m = C.m, n = C.n;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= C.ns) return;
@@ -169,9 +189,11 @@ __global__ void k_adj_coarsifyT(const DevCase* __restrict__ cases, const AdjCase
   A.aW[(size_t)(k - 2) * C.ns + t] += s;
 }
 
-__global__ void k_adj_zero_centre(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adj_zero_centre(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids, int k) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  if (k > C.L) return;
   int m = C.m, n = C.n;
   int ci = 3 * m / 4 - (m / 4 + 2) + 1, cj = 3 * n / 4 - (n / 4 + 2) + 1;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -208,9 +230,10 @@ __device__ __forceinline__ double regT_curl0(const DevCase& C, const double* __r
 // operators.f90:174) ; objective: J += wx_b fx_b + wy_b fy_b with
 // f = 2 delta / dt * sum wsum_f fb_f (write_force; a moving body's wsum is
 // the sum of its current weights).
-__global__ void k_adj_force(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adj_force(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= C.nf) return;
   int p = f < C.nb ? f : f - C.nb;
@@ -220,9 +243,14 @@ __global__ void k_adj_force(const DevCase* __restrict__ cases, const AdjCase* __
   A.aF[f] = v - regT_curl0(C, A.aZ1, f);
 }
 
-// y = Linv b (lower) / x = LinvT y (upper) on adjoint vectors; warp per row.
-__global__ void k_adj_tri(const DevCase* __restrict__ cases, const double* __restrict__ in, double* out, int upper) {
-  const DevCase& C = cases[0];
+// aTmp = Linv aF (lower) / aRf = LinvT aTmp (upper) on adjoint vectors; warp per row.
+__global__ void k_adj_tri(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
+                          const int* __restrict__ cids, int upper) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  const double* in = upper ? A.aTmp : A.aF;
+  double* out = upper ? A.aRf : A.aTmp;
   int nf = C.nf;
   int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
   if (row >= nf) return;
@@ -237,9 +265,10 @@ __global__ void k_adj_tri(const DevCase* __restrict__ cases, const double* __res
 
 // q1_hat = reg(rhsf_hat) on all faces; grad_vel -= delta * rhsf_hat
 // (rhsf = regT(q1) - (delta*vel - regT(q0)), operators.f90:155-164).
-__global__ void k_adj_rhsf(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adj_rhsf(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < C.nq) A.aQ1[t] = reg_face(C, A.aRf, t);
   if (t < C.nf) A.aGrad[t] -= C.delta * A.aRf[t];
@@ -253,21 +282,23 @@ __global__ void k_adj_rhsf(const DevCase* __restrict__ cases, const AdjCase* __r
 // smearing weights with respect to the body positions.
 
 // aQ1 = reg(x) on all faces (the first operator of A^T).
-__global__ void k_adjm_reg_in(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
-                              const double* __restrict__ x) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adjm_reg_in(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids,
+                              const double* const* __restrict__ xs) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < C.nq) A.aQ1[t] = reg_face(C, x, t);
+  if (t < C.nq) A.aQ1[t] = reg_face(C, xs[slot], t);
 }
 
 // out = regT(curl(aZ1, 0)) (the last two operators of A^T).
-__global__ void k_adjm_regT_curl0(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
-                                  double* __restrict__ out) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adjm_regT_curl0(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids,
+                                  double* const* __restrict__ outs) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
   int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f < C.nf) out[f] = regT_curl0(C, A.aZ1, f);
+  if (f < C.nf) outs[slot][f] = regT_curl0(C, A.aZ1, f);
 }
 
 // One step's contribution to dJ/d(pitch amplitude, radians), added to *acc.
@@ -286,11 +317,15 @@ __global__ void k_adjm_regT_curl0(const DevCase* __restrict__ cases, const AdjCa
 //   dV/dA from both d thetadot/dA = -Om cos(Om t) and dX/dA, dY/dA;
 // the velocity enters rhsf as -dx V, so dJ/dV_f = -dx b-hat_f.
 // One block; the points are reduced in a fixed order.
-__global__ void k_adjm_position(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj,
-                                const double* __restrict__ zcg, const double* __restrict__ u,
-                                double* __restrict__ acc) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adjm_position(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids,
+                                const AdjCase* __restrict__ acg, const double* const* __restrict__ us,
+                                double* __restrict__ accs) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  const double* __restrict__ zcg = acg[slot].aZ1;
+  const double* __restrict__ u = us[slot];
+  double* acc = accs + slot;
   const int m = C.m, n = C.n, nb = C.nb;
   const double dx = C.delta, d2 = 0.5 * dx;
   const double t = C.dt * (double)(*C.itime);
@@ -345,9 +380,11 @@ __global__ void k_adjm_position(const DevCase* __restrict__ cases, const AdjCase
 // Level-k CN adjoint, node part: r_hat = con1 A_hat + P_hat' ; P_hat = con2 A_hat
 // (first step: rhs_old was set to rhs, so r_hat += con2 A_hat, P_hat = 0);
 // ring part: lastbc_hat_k += vfac apply_bc^T(A_hat), ob_hat = vfac apply_bc^T(A_hat).
-__global__ void k_adj_level(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k, int first) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adj_level(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids, int k, int first) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  if (k > C.L) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   double del22 = C.delta * C.delta * (double)(1 << (2 * (k - 1)));
   double con1 = 1.5 * C.dt / del22 / C.norm, con2 = -0.5 * C.dt / del22 / C.norm;
@@ -373,9 +410,11 @@ __global__ void k_adj_level(const DevCase* __restrict__ cases, const AdjCase* __
 //   node  omega_hat(i,j) += .5 va(i,j)(Hu(i,j-1)+Hu(i,j)) - .5 ua(i,j)(Hv(i-1,j)+Hv(i,j))
 //   ring  lastbc_hat     += the same products at the edge entries
 //   face  q_hat           = .5 * (adjoints of the face averages uavg / vavg)
-__global__ void k_adj_nonlinear(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, int k) {
-  const DevCase& C = cases[0];
-  const AdjCase& A = adj[0];
+__global__ void k_adj_nonlinear(const DevCase* __restrict__ cases, const AdjCase* __restrict__ adj, const int* __restrict__ cids, int k) {
+  const int slot = blockIdx.z;
+  const DevCase& C = cases[cids[slot]];
+  const AdjCase& A = adj[slot];
+  if (k > C.L) return;
   int m = C.m, n = C.n;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const double* W = A.fwW + (size_t)(k - 1) * C.ns;
@@ -443,45 +482,46 @@ __global__ void k_adj_nonlinear(const DevCase* __restrict__ cases, const AdjCase
 }
 
 // -------------------------------------------------------------------------
-void adj_curlT(const DevCase* c, const AdjCase* a, const DevCase& h, int nlev, int use_q1, cudaStream_t st) {
-  k_adj_curlT<<<dim3((h.ns + h.nring + 255) / 256, h.L), 256, 0, st>>>(c, a, nlev, use_q1);
+static dim3 grid_of(int count, int threads, const AdjGroup& g, int gy = 1) {
+  return dim3((count + threads - 1) / threads, gy, g.n);
 }
-void adj_v2f_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st) {
-  k_adj_v2f_level<<<(h.ns + h.nring + 255) / 256, 256, 0, st>>>(c, a, k);
+void adj_curlT(const AdjGroup& g, int nlev, int use_q1, cudaStream_t st) {
+  k_adj_curlT<<<grid_of(g.max_ns + g.max_ring, 256, g, g.max_L), 256, 0, st>>>(g.dc, g.da, g.cids, nlev, use_q1);
 }
-void adj_getbcT(const DevCase* c, const double* ring, double* dst, const DevCase& h, double fac, cudaStream_t st) {
-  int np = 2 * (h.m / 2 + 1) + 2 * (h.n / 2 - 1);
-  k_adj_getbcT<<<(np + 255) / 256, 256, 0, st>>>(c, ring, dst, fac);
+void adj_v2f_level(const AdjGroup& g, int k, cudaStream_t st) {
+  k_adj_v2f_level<<<grid_of(g.max_ns + g.max_ring, 256, g), 256, 0, st>>>(g.dc, g.da, g.cids, k);
 }
-void adj_coarsifyT(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st) {
-  k_adj_coarsifyT<<<(h.ns + 255) / 256, 256, 0, st>>>(c, a, k);
-  k_adj_zero_centre<<<(h.ns / 4 + 255) / 256 + 1, 256, 0, st>>>(c, a, k);
+void adj_getbcT(const AdjGroup& g, int which, int k, double fac, cudaStream_t st) {
+  k_adj_getbcT<<<grid_of(g.max_perim, 256, g), 256, 0, st>>>(g.dc, g.da, g.cids, which, k, fac);
 }
-void adj_force(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st) {
-  k_adj_force<<<(h.nf + 127) / 128, 128, 0, st>>>(c, a);
+void adj_coarsifyT(const AdjGroup& g, int k, cudaStream_t st) {
+  k_adj_coarsifyT<<<grid_of(g.max_ns, 256, g), 256, 0, st>>>(g.dc, g.da, g.cids, k);
+  k_adj_zero_centre<<<grid_of(g.max_ns / 4 + 256, 256, g), 256, 0, st>>>(g.dc, g.da, g.cids, k);
 }
-void adj_solve(const DevCase* c, const double* in, double* tmp, double* out, const DevCase& h, cudaStream_t st) {
-  k_adj_tri<<<(h.nf + 7) / 8, 256, 0, st>>>(c, in, tmp, 0);
-  k_adj_tri<<<(h.nf + 7) / 8, 256, 0, st>>>(c, tmp, out, 1);
+void adj_force(const AdjGroup& g, cudaStream_t st) {
+  k_adj_force<<<grid_of(g.max_nf, 128, g), 128, 0, st>>>(g.dc, g.da, g.cids);
 }
-void adj_rhsf(const DevCase* c, const AdjCase* a, const DevCase& h, cudaStream_t st) {
-  k_adj_rhsf<<<(h.nq + 255) / 256, 256, 0, st>>>(c, a);
+void adj_solve(const AdjGroup& g, cudaStream_t st) {
+  k_adj_tri<<<grid_of(g.max_nf, 8, g), 256, 0, st>>>(g.dc, g.da, g.cids, 0);
+  k_adj_tri<<<grid_of(g.max_nf, 8, g), 256, 0, st>>>(g.dc, g.da, g.cids, 1);
 }
-void adjm_reg_in(const DevCase* c, const AdjCase* a, const double* x, const DevCase& h, cudaStream_t st) {
-  k_adjm_reg_in<<<(h.nq + 255) / 256, 256, 0, st>>>(c, a, x);
+void adj_rhsf(const AdjGroup& g, cudaStream_t st) {
+  k_adj_rhsf<<<grid_of(std::max(g.max_nq, g.max_nf), 256, g), 256, 0, st>>>(g.dc, g.da, g.cids);
 }
-void adjm_regT_curl0(const DevCase* c, const AdjCase* a, double* out, const DevCase& h, cudaStream_t st) {
-  k_adjm_regT_curl0<<<(h.nf + 127) / 128, 128, 0, st>>>(c, a, out);
+void adjm_reg_in(const AdjGroup& g, const double* const* xs, cudaStream_t st) {
+  k_adjm_reg_in<<<grid_of(g.max_nq, 256, g), 256, 0, st>>>(g.dc, g.da, g.cids, xs);
 }
-void adjm_position(const DevCase* c, const AdjCase* a, const double* zcg, const double* u, double* acc,
-                   cudaStream_t st) {
-  k_adjm_position<<<1, 128, 0, st>>>(c, a, zcg, u, acc);
+void adjm_regT_curl0(const AdjGroup& g, double* const* outs, cudaStream_t st) {
+  k_adjm_regT_curl0<<<grid_of(g.max_nf, 128, g), 128, 0, st>>>(g.dc, g.da, g.cids, outs);
 }
-void adj_level(const DevCase* c, const AdjCase* a, const DevCase& h, int k, int first, cudaStream_t st) {
-  k_adj_level<<<(h.ns + h.nring + 255) / 256, 256, 0, st>>>(c, a, k, first);
+void adjm_position(const AdjGroup& g, const AdjCase* acg, const double* const* us, double* accs, cudaStream_t st) {
+  k_adjm_position<<<dim3(1, 1, g.n), 128, 0, st>>>(g.dc, g.da, g.cids, acg, us, accs);
 }
-void adj_nonlinear(const DevCase* c, const AdjCase* a, const DevCase& h, int k, cudaStream_t st) {
-  k_adj_nonlinear<<<(h.ns + h.nq + h.nring + 255) / 256, 256, 0, st>>>(c, a, k);
+void adj_level(const AdjGroup& g, int k, int first, cudaStream_t st) {
+  k_adj_level<<<grid_of(g.max_ns + g.max_ring, 256, g), 256, 0, st>>>(g.dc, g.da, g.cids, k, first);
+}
+void adj_nonlinear(const AdjGroup& g, int k, cudaStream_t st) {
+  k_adj_nonlinear<<<grid_of(g.max_ns + g.max_nq + g.max_ring, 256, g), 256, 0, st>>>(g.dc, g.da, g.cids, k);
 }
 
 }  // namespace ibfs

@@ -274,17 +274,25 @@ class Solver:
                                              _p(col["u_j_osc"]), _p(col["omg_j"]), _p(col["theta_j"])))
 
     def adjoint_pitch_run(self, nsteps, checkpoint_every, wx, wy):
-        """J and dJ/d(pitch amplitude, per degree) over nsteps advances of a
-        single pitching case (see ibfs_adjoint_pitch_run)."""
-        wx = np.ascontiguousarray(wx, dtype=np.float64)
-        wy = np.ascontiguousarray(wy, dtype=np.float64)
-        J, dJ = ctypes.c_double(), ctypes.c_double()
+        """J and dJ/d(pitch amplitude, per degree) over nsteps advances of the
+        handle's pitching cases (see ibfs_adjoint_pitch_run). wx, wy: per case
+        nsteps x nbody weights, case-major; a 1-D array of nsteps applies to
+        every case (one body each). Scalars for a single case, arrays for a
+        batch."""
+        nc = self.ncases
+        wx = np.asarray(wx, dtype=np.float64)
+        wy = np.asarray(wy, dtype=np.float64)
+        if wx.ndim == 1 and nc > 1:
+            wx, wy = np.tile(wx, nc), np.tile(wy, nc)
+        wx, wy = np.ascontiguousarray(wx.ravel()), np.ascontiguousarray(wy.ravel())
+        J, dJ = np.zeros(nc), np.zeros(nc)
         ms_f, ms_t = ctypes.c_double(), ctypes.c_double()
-        self._check(lib().ibfs_adjoint_pitch_run(self.h, nsteps, checkpoint_every, _p(wx), _p(wy), ctypes.byref(J),
-                                                 ctypes.byref(dJ), ctypes.byref(ms_f), ctypes.byref(ms_t)),
-                    step=True)
+        self._check(lib().ibfs_adjoint_pitch_run(self.h, nsteps, checkpoint_every, _p(wx), _p(wy), _p(J), _p(dJ),
+                                                 ctypes.byref(ms_f), ctypes.byref(ms_t)), step=True)
         self.itime.value += nsteps
-        return J.value, dJ.value, ms_f.value, ms_t.value
+        if nc == 1:
+            return float(J[0]), float(dJ[0]), ms_f.value, ms_t.value
+        return J, dJ, ms_f.value, ms_t.value
 
     def last_cg_iterations(self):
         return lib().ibfs_last_cg_iterations(self.h)

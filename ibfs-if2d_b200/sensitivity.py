@@ -2,8 +2,8 @@
 amplitude.
 
 mean_drag_amplitude_adjoint: the discrete adjoint (ibfs_adjoint_pitch_run),
-one single-case handle per amplitude; the cost is about three forward solves
-of that case whatever the number of parameters the objective is taken over.
+all amplitudes differentiated together as the cases of one handle; the cost
+is about three forward solves of the batch.
 
 mean_drag_amplitude_derivative: central differences inside one batched run
 (every amplitude A becomes the two cases A - h and A + h, advanced together),
@@ -16,19 +16,31 @@ import ibfs_capi as C
 import workloads as W
 
 
-def mean_drag_amplitude_adjoint(amps_deg, steps=100, tail=None, checkpoint_every=50, workers=1, **case_kw):
+def mean_drag_amplitude_adjoint(amps_deg, steps=100, tail=None, checkpoint_every=50, batched=True, workers=1,
+                                **case_kw):
     """J(A) and dJ/dA (per degree) for each amplitude in amps_deg by the
-    discrete adjoint; case_kw as for workloads.pitching. With workers > 1 the
-    single-case adjoints run from that many host threads at once, each handle
-    on its own stream (the library releases no shared state between handles;
+    discrete adjoint; case_kw as for workloads.pitching. batched: every
+    amplitude is a case of one handle and all are differentiated together
+    (one launch per stage). Otherwise one handle per amplitude; with
+    workers > 1 those single-case adjoints run from that many host threads at
+    once, each handle on its own stream (handles share no mutable state;
     results are bit-identical to a sequential run)."""
     tail = steps if tail is None else int(tail)
     wx = np.zeros(steps)
     wx[steps - tail:] = 1.0 / tail
     wy = np.zeros(steps)
+    cases = [W.pitching(amp_deg=float(a), **case_kw) for a in np.asarray(amps_deg, dtype=np.float64)]
+    if batched:
+        params, bodies, opts = W.solver_args(cases, C)
+        g = C.Solver(params, bodies, opts)
+        try:
+            J, d, _, _ = g.adjoint_pitch_run(steps, checkpoint_every, wx, wy)
+        finally:
+            g.close()
+        return np.atleast_1d(J), np.atleast_1d(d)
     solvers = []
-    for a in np.asarray(amps_deg, dtype=np.float64):
-        params, bodies, opts = W.solver_args([W.pitching(amp_deg=float(a), **case_kw)], C)
+    for c in cases:
+        params, bodies, opts = W.solver_args([c], C)
         solvers.append(C.Solver(params[0], bodies[0], opts[0]))
 
     def run(s):

@@ -190,22 +190,25 @@ int ibfs_adjoint_run(ibfs_handle* h, int nsteps, int checkpoint_every, const dou
 int ibfs_set_actuators(ibfs_handle* h, int icase, int n_act, const int* npt, const double* u_j,
                        const double* u_j_osc, const double* omg_j, const double* theta_j);
 
-/* Discrete adjoint of nsteps advances of a single rigidly pitching body (no
- * reference counterpart): motion_kind 1, stationary = .FALSE. (CG force
- * solve, cjgr operators.f90:393-441), plain FP64 form. From the current state
- * it runs nsteps advances and returns J = sum_s sum_b (wx[s*nbody+b] fx_b^s +
- * wy[s*nbody+b] fy_b^s) and dJ_damp = dJ / d(pitch_amp_deg), per degree of
- * amplitude. The amplitude moves the body points (the regularisation weights
- * of reg/regT, setup_reg grid.f90:142-230, differentiated through the
- * Roma-Peskin-Berger kernel, grid.f90:233-249) and sets their velocities
- * (the right-hand side of the force system). The CG solve is differentiated
- * as an exact solve: its adjoint is a CG solve with the transposed force
- * operator, stopped by the same tolerance rule. Checkpoints every
- * checkpoint_every steps as ibfs_adjoint_run. On return the state is the
- * state after the nsteps advances; ibfs_last_cg_iterations reports the
- * largest adjoint CG iteration count. Returns IBFS_ERR_CG_MAXITER (a
- * warning, results valid) when a forward or adjoint solve used
- * cg_max_iter iterations. */
+/* Discrete adjoint of nsteps advances of rigidly pitching bodies (no
+ * reference counterpart): every case of the handle has motion_kind 1,
+ * stationary = .FALSE. (CG force solve, cjgr operators.f90:393-441) and the
+ * plain FP64 form, and all are at the same step. From the current states it
+ * runs nsteps advances of the handle and returns, per case c,
+ * J[c] = sum_s sum_b (wx[c][s][b] fx_b^s + wy[c][s][b] fy_b^s) and
+ * dJ_damp[c] = dJ[c] / d(pitch_amp_deg of case c), per degree of amplitude;
+ * wx and wy are case-major, nsteps x nbody(c) values per case. The cases are
+ * differentiated together, one launch per stage for all of them. The
+ * amplitude moves the body points (the regularisation weights of reg/regT,
+ * setup_reg grid.f90:142-230, differentiated through the Roma-Peskin-Berger
+ * kernel, grid.f90:233-249) and sets their velocities (the right-hand side of
+ * the force system). The CG solve is differentiated as an exact solve: its
+ * adjoint is a CG solve with the transposed force operator, stopped by the
+ * same tolerance rule. Checkpoints every checkpoint_every steps as
+ * ibfs_adjoint_run. On return the states are those after the nsteps
+ * advances; ibfs_last_cg_iterations reports the largest adjoint CG iteration
+ * count. Returns IBFS_ERR_CG_MAXITER (a warning, results valid) when a
+ * forward or adjoint solve used cg_max_iter iterations. */
 int ibfs_adjoint_pitch_run(ibfs_handle* h, int nsteps, int checkpoint_every, const double* wx, const double* wy,
                            double* J, double* dJ_damp, double* ms_forward, double* ms_total);
 

@@ -67,3 +67,23 @@ def test_pitch_adjoint_vs_tangent_linear_and_state():
     ref = s.get_state()
     s.close()
     assert np.array_equal(st["omega"], ref["omega"]) and np.array_equal(st["fb"], ref["fb"])
+
+
+def test_pitch_adjoint_batched_equals_single():
+    """Several amplitudes (and grids) differentiated together, one slot each,
+    give each case's single-handle J and dJ/dA."""
+    kw2 = dict(KW, m=32, levels=2)
+    cases = [W.pitching(amp_deg=a, **KW) for a in (8.0, 21.0)] + [W.pitching(amp_deg=14.0, **kw2)]
+    p, b, o = W.solver_args(cases, C)
+    g = C.Solver(p, b, o)
+    wx = np.zeros(STEPS)
+    wx[STEPS - TAIL:] = 1.0 / TAIL
+    Jb, gb, ms_f, ms_t = g.adjoint_pitch_run(STEPS, 5, wx, np.zeros(STEPS))
+    assert Jb.shape == (3,) and gb.shape == (3,)
+    for i in range(3):
+        s = C.Solver(p[i], b[i], o[i])
+        Js, gs, _, _ = s.adjoint_pitch_run(STEPS, 5, wx, np.zeros(STEPS))
+        s.close()
+        assert abs(Jb[i] - Js) <= 1e-13 * abs(Js), i
+        assert abs(gb[i] - gs) <= 1e-11 * abs(gs), (i, gb[i], gs)
+    g.close()
