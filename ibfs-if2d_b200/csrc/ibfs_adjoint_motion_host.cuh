@@ -16,7 +16,8 @@
 //   b-hat = A^-T fb-hat,  A = regT M reg,  A^T = regT M^T reg,
 // solved by CG with the same kernels on views of the cases whose right-hand
 // side is fb-hat and whose solution is b-hat (warm-started from the previous
-// step's b-hat; converged slots idle), A^T applied with the transposed
+// step's b-hat; converged slots idle; preconditioned like the forward solve
+// when the case is, the preconditioner being symmetric), A^T applied with the transposed
 // operators of the stationary adjoint. The position derivative needs, per
 // step, fb_s, the flux q1 + q0 at each force's faces (captured by the forward
 // rhsf kernel), u = M reg fb_s (one forward a_times) and v = M^T reg b-hat
@@ -93,9 +94,11 @@ static int adjm_init(ibfs_handle* h, AdjPlan& P, AdjMPlan& M) {
     v.cg_d = dalloc<double>(h, v.nf);
     v.cg_q = dalloc<double>(h, v.nf);
     v.cg_q2 = dalloc<double>(h, v.nf);
-    v.cg_sc = dalloc<double>(h, 4);
+    v.cg_z = dalloc<double>(h, v.nf);
+    v.cg_y = dalloc<double>(h, v.nf);
+    v.cg_sc = dalloc<double>(h, 5);
     v.cg_it = M.d_vit + 2 * i;
-    ok = v.cg_r && v.cg_d && v.cg_q && v.cg_q2 && v.cg_sc;
+    ok = v.cg_r && v.cg_d && v.cg_q && v.cg_q2 && v.cg_z && v.cg_y && v.cg_sc;
     M.vc.push_back(v);
     xs_fb.push_back(v.fb);
     xs_d.push_back(v.cg_d);
@@ -216,7 +219,8 @@ static int adjm_run(ibfs_handle* h, int nsteps, int K, const double* wx, const d
     if (c.itime != h->cases[0].itime) return set_error(IBFS_ERR_ARG, "the pitch adjoint needs every case at the same step");
   }
   if (nsteps < 1 || K < 1 || !wx || !wy || !J || !dJdA) return set_error(IBFS_ERR_ARG, "bad adjoint arguments");
-  int rc = IBFS_OK, warn = IBFS_OK;
+  int rc = precompute(h), warn = IBFS_OK;  // the preconditioners' factors, if any
+  if (rc) return rc;
   if (!h->adj) {
     std::vector<int> all(n);
     for (int i = 0; i < n; i++) all[i] = i;

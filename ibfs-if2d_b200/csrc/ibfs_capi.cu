@@ -597,7 +597,13 @@ static int run_step(ibfs_handle* h) {
 }
 
 // ---------------------------------------------------------------------------
-// preprocess (operators.f90:29-59) for every stationary case lacking a factor:
+// A case needs the factor of its force operator: stationary bodies for the
+// Cholesky solve, preconditioned CG cases for the preconditioner.
+static bool needs_factor(const HostCase& c) {
+  return (c.p.stationary || c.dc.cg_pre) && !c.have_chol && c.nf > 0;
+}
+
+// preprocess (operators.f90:29-59) for every case lacking a factor:
 // the columns a_times(e_j) of all such cases are computed as "shadow cases"
 // (one per right-hand side, sharing the real case's grid tables, with private
 // scratch), packed from any mix of cases into chunks of a fixed memory budget
@@ -605,8 +611,22 @@ static int run_step(ibfs_handle* h) {
 static int precompute(ibfs_handle* h) {
   std::vector<int> need;
   for (size_t i = 0; i < h->cases.size(); i++)
-    if (h->cases[i].p.stationary && !h->cases[i].have_chol && h->cases[i].nf > 0) need.push_back((int)i);
+    if (needs_factor(h->cases[i])) need.push_back((int)i);
   if (need.empty()) return IBFS_OK;
+  // a preconditioned moving body is factored at its zero-pitch positions:
+  // the regularisation tables are rebuilt there (every step rebuilds its own)
+  std::vector<int> mv;
+  for (int ci : need)
+    if (h->cases[ci].dc.moving) mv.push_back(ci);
+  if (!mv.empty()) {
+    for (int ci : mv) {
+      const DevCase& d = h->cases[ci].dc;
+      IBFS_CUDA_CHECK(cudaMemcpyAsync(d.xb, d.xb0, sizeof(double) * d.nb, cudaMemcpyDeviceToDevice, h->st));
+      IBFS_CUDA_CHECK(cudaMemcpyAsync(d.yb, d.yb0, sizeof(double) * d.nb, cudaMemcpyDeviceToDevice, h->st));
+    }
+    int* dmv = dupload(h, mv);
+    launch_setup_reg_moving(h->d_cases, dmv, (int)mv.size(), h->max_nf, h->max_patch, h->st);
+  }
   const size_t budget = (size_t)4 << 30;
   auto per_rhs = [&](const DevCase& c) {
     size_t nsL = (size_t)c.L * c.ns;
@@ -822,7 +842,10 @@ static int setup_case(ibfs_handle* h, HostCase& c, const ibfs_params_c& p, const
     d.cg_d = dalloc<double>(h, c.nf);
     d.cg_q = dalloc<double>(h, c.nf);
     d.cg_q2 = dalloc<double>(h, c.nf);
-    d.cg_sc = dalloc<double>(h, 4);
+    d.cg_z = dalloc<double>(h, c.nf);
+    d.cg_y = dalloc<double>(h, c.nf);
+    d.cg_sc = dalloc<double>(h, 5);
+    d.cg_pre = c.o.cg_precond ? 1 : 0;
     d.cgtol = p.cgtol;
     d.cg_max_iter = p.cg_max_iter;
     d.cg_rel = c.o.cg_relative;
@@ -1123,7 +1146,7 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
   }
   // preprocess at the first step (operators.f90:88-90), unless the caller
   // supplied the factor (the reference reads input/ibfs.chd then, :44-46)
-  if (c.p.stationary && !c.have_chol) {
+  if (needs_factor(c)) {
     int rc = precompute(h);
     if (rc) { h->err = t_error; return rc; }
   }
@@ -1153,7 +1176,7 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
 int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out) {
   if (!h) return IBFS_ERR_ARG;
   bool need = false;
-  for (auto& c : h->cases) if (c.p.stationary && !c.have_chol) need = true;
+  for (auto& c : h->cases) if (needs_factor(c)) need = true;
   if (need) {
     int rc = precompute(h);
     if (rc) { h->err = t_error; return rc; }
@@ -1180,7 +1203,7 @@ int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out) {
 int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist) {
   if (!h || nsteps < 0) return IBFS_ERR_ARG;
   bool need = false;
-  for (auto& c : h->cases) if (c.p.stationary && !c.have_chol) need = true;
+  for (auto& c : h->cases) if (needs_factor(c)) need = true;
   if (need) {
     int rc = precompute(h);
     if (rc) { h->err = t_error; return rc; }

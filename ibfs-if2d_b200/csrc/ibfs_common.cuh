@@ -73,7 +73,9 @@ struct DevCase {
 
   // conjugate gradient (operators.f90:393-441) on the force system
   double *cg_r, *cg_d, *cg_q, *cg_q2;  // [Nf]
-  double* cg_sc;                       // delta_new, delta_old, eps, alpha
+  double *cg_z, *cg_y;                 // [Nf] preconditioned residual and its half-solve (cg_pre)
+  double* cg_sc;                       // delta_new (r.z), delta_old, eps, alpha, r.r
+  int cg_pre;                          // preconditioned by the zero-pitch factor (Linv, LinvT)
   int* cg_it;                          // iterations, active flag
   double cgtol;
   int cg_max_iter, cg_rel;

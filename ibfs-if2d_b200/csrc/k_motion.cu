@@ -121,7 +121,8 @@ __global__ void k_setup_reg_patch(const DevCase* __restrict__ cases, const int* 
 // --------------------------------------------------------------------------
 // CG (operators.f90:393-441), one CTA per case, FP64 reductions in a fixed
 // order (block tree). Scalars: sc[0] delta_new, sc[1] delta_old, sc[2] eps,
-// sc[3] alpha; it[0] iterations, it[1] active.
+// sc[3] alpha, sc[4] r.r of the preconditioned form; it[0] iterations,
+// it[1] active.
 __device__ double block_dot(const double* a, const double* b, int n, double* red) {
   double s = 0.0;
   for (int t = threadIdx.x; t < n; t += blockDim.x) s = fma(a[t], b[t], s);
@@ -136,11 +137,79 @@ __device__ double block_dot(const double* a, const double* b, int n, double* red
   return r;
 }
 
-// r = b - A x (A x in cg_q), d = r, delta_new = r.r, eps, active.
+// z = P r = Q L0^-T L0^-1 Q^T r (one CTA): the force operator factored at the
+// zero-pitch body, A0 = L0 L0^T (Linv = L0^-1 and LinvT, row-major), applied
+// in the body frame of this step. A rigid rotation by theta moves every
+// point's force pair with it, so A(theta) ~ Q A0 Q^T up to the grid's
+// anisotropy, Q the rotation of each (fx_k, fy_k); theta = 0 for a body that
+// does not move. The triangular products run one warp per row, in a fixed
+// order.
+__device__ void cg_precond(const DevCase& C, const double* __restrict__ r, double* __restrict__ z) {
+  const int nb = C.nb, nf = C.nf;
+  double c = 1.0, s = 0.0;
+  if (C.moving) {
+    double th = -(C.pitch_amp * sin(C.pitch_omega * (C.dt * (double)(*C.itime))));
+    c = cos(th);
+    s = sin(th);
+  }
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {  // Q^T r
+    double rx = r[k], ry = r[nb + k];
+    z[k] = c * rx + s * ry;
+    z[nb + k] = -s * rx + c * ry;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  double* y = C.cg_y;
+  for (int row = warp; row < nf; row += nw) {  // y = L0^-1 (Q^T r)
+    const double* Mr = C.Linv + (size_t)row * nf;
+    double a = 0.0;
+    for (int k = lane; k <= row; k += 32) a = fma(Mr[k], z[k], a);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) y[row] = a;
+  }
+  __syncthreads();
+  for (int row = warp; row < nf; row += nw) {  // L0^-T y
+    const double* Mr = C.LinvT + (size_t)row * nf;
+    double a = 0.0;
+    for (int k = row + lane; k < nf; k += 32) a = fma(Mr[k], y[k], a);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) z[row] = a;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {  // Q (...)
+    double wx = z[k], wy = z[nb + k];
+    z[k] = c * wx - s * wy;
+    z[nb + k] = s * wx + c * wy;
+  }
+  __syncthreads();
+}
+
+// r = b - A x (A x in cg_q), d = r, delta_new = r.r, eps, active
+// (preconditioned: z = P r, d = z, delta_new = r.z; the stop test stays r.r).
 __global__ void k_cg_start(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
   const DevCase& C = cases[cids[blockIdx.x]];
   __shared__ double red[256];
   int nf = C.nf;
+  if (C.cg_pre) {
+    for (int t = threadIdx.x; t < nf; t += blockDim.x) C.cg_r[t] = C.rhsf[t] - C.cg_q[t];
+    __syncthreads();
+    double rr = block_dot(C.cg_r, C.cg_r, nf, red);
+    cg_precond(C, C.cg_r, C.cg_z);
+    for (int t = threadIdx.x; t < nf; t += blockDim.x) C.cg_d[t] = C.cg_z[t];
+    double rz = block_dot(C.cg_r, C.cg_z, nf, red);
+    double eps = C.cgtol * C.cgtol;
+    if (C.cg_rel) eps = eps * block_dot(C.rhsf, C.rhsf, nf, red);
+    if (threadIdx.x == 0) {
+      C.cg_sc[0] = rz;
+      C.cg_sc[2] = eps;
+      C.cg_sc[4] = rr;
+      C.cg_it[0] = 0;
+      C.cg_it[1] = (C.cg_max_iter > 0 && rr > eps) ? 1 : 0;
+    }
+    return;
+  }
   for (int t = threadIdx.x; t < nf; t += blockDim.x) {
     double r = C.rhsf[t] - C.cg_q[t];
     C.cg_r[t] = r;
@@ -180,12 +249,30 @@ __global__ void k_cg_resid(const DevCase* __restrict__ cases, const int* __restr
   for (int t = threadIdx.x; t < C.nf; t += blockDim.x) C.cg_r[t] = C.rhsf[t] - C.cg_q2[t];
 }
 
-// delta_old = delta_new; delta_new = r.r; d = r + beta d; iter++; active.
+// delta_old = delta_new; delta_new = r.r; d = r + beta d; iter++; active
+// (preconditioned: z = P r, delta_new = r.z, d = z + beta d, stop on r.r).
 __global__ void k_cg_beta(const DevCase* __restrict__ cases, const int* __restrict__ cids) {
   const DevCase& C = cases[cids[blockIdx.x]];
   if (!C.cg_it[1]) return;
   __shared__ double red[256];
   int nf = C.nf;
+  if (C.cg_pre) {
+    double rr = block_dot(C.cg_r, C.cg_r, nf, red);
+    cg_precond(C, C.cg_r, C.cg_z);
+    double rz = block_dot(C.cg_r, C.cg_z, nf, red);
+    double beta = rz / C.cg_sc[0];
+    for (int t = threadIdx.x; t < nf; t += blockDim.x) C.cg_d[t] = C.cg_z[t] + beta * C.cg_d[t];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      C.cg_sc[1] = C.cg_sc[0];
+      C.cg_sc[0] = rz;
+      C.cg_sc[4] = rr;
+      int it = C.cg_it[0] + 1;
+      C.cg_it[0] = it;
+      C.cg_it[1] = (it < C.cg_max_iter && rr > C.cg_sc[2]) ? 1 : 0;
+    }
+    return;
+  }
   double dn = block_dot(C.cg_r, C.cg_r, nf, red);
   double beta = dn / C.cg_sc[0];
   for (int t = threadIdx.x; t < nf; t += blockDim.x) C.cg_d[t] = C.cg_r[t] + beta * C.cg_d[t];

@@ -35,6 +35,7 @@ MODULE ibfs_gpu
      INTEGER(C_INT) :: precision, cg_relative, motion_kind
      REAL(C_DOUBLE) :: pitch_amp_deg, pitch_freq, pivot_x, pivot_y
      INTEGER(C_INT) :: tile_cfg
+     INTEGER(C_INT) :: cg_precond
   END TYPE ibfs_options_c
 
   INTERFACE

@@ -36,7 +36,7 @@ PROGRAM main_gpu
   ! THE GPU CASE: same parameters, same body points, same initial state
   p = ibfs_params_c(istart, istop, isave, m, n, dt, Re, cgtol, cg_max_iter, MERGE(1, 0, unif_flow), &
                     len, offsetx, offsety, mgridlev, MERGE(1, 0, make_vortex), MERGE(1, 0, stationary))
-  opt = ibfs_options_c(0, 0, 0, 0.d0, 0.d0, 0.d0, 0.d0, -1)
+  opt = ibfs_options_c(0, 0, 0, 0.d0, 0.d0, 0.d0, 0.d0, -1, 0)
   rc = ibfs_create(p, opt, INT(nb, C_INT), xb, yb, INT(bdyno, C_INT), h)
   CALL ibfs_stop_on(rc, h)
   rc = ibfs_case_sizes(h, 0_C_INT, gm, gn, glev, gnq, gnb, gnbody)

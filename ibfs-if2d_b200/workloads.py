@@ -98,12 +98,14 @@ def shard(cases, rank, world):
     return [i for i in range(len(cases)) if owner[i] == rank]
 
 
-def pitching(m=512, levels=5, re=500.0, dt=0.001, amp_deg=20.0, freq=0.25, cgtol=1e-12):
+def pitching(m=512, levels=5, re=500.0, dt=0.001, amp_deg=20.0, freq=0.25, cgtol=1e-12, precond=True):
     """Flat plate of chord 1 pitching sinusoidally about mid-chord,
     alpha(t) = amp sin(2 pi freq t), body points at spacing dx along the chord;
-    the force system is solved by CG to a relative residual of cgtol every step."""
+    the force system is solved by CG to a relative residual of cgtol every step
+    (preconditioned by the zero-pitch factor turned with the plate unless
+    precond is False)."""
     c = case(m, levels, re, dt, "plate", aoa=0.0)
-    c.update(pitch_amp_deg=float(amp_deg), pitch_freq=float(freq), cgtol=float(cgtol))
+    c.update(pitch_amp_deg=float(amp_deg), pitch_freq=float(freq), cgtol=float(cgtol), cg_precond=int(bool(precond)))
     return c
 
 
@@ -122,7 +124,8 @@ def solver_args(cases, capi, precision=0):
             params.append(capi.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"], stationary=False,
                                            cgtol=c["cgtol"]))
             opts.append(capi.make_options(precision=precision, cg_relative=1, motion_kind=1,
-                                          pitch_amp_deg=c["pitch_amp_deg"], pitch_freq=c["pitch_freq"]))
+                                          pitch_amp_deg=c["pitch_amp_deg"], pitch_freq=c["pitch_freq"],
+                                          cg_precond=c.get("cg_precond", 0)))
         else:
             params.append(capi.make_params(c["m"], c["n"], c["dt"], c["re"], c["levels"]))
             opts.append(capi.make_options(precision=precision))
