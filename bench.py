@@ -275,12 +275,46 @@ def plain_and_split_plate(C, torch, steps, warmup, flush):
     return plain, split
 
 
+MAX_PITCH_STEP = 1000  # t = 1/(4 f) = 1 s at dt 0.001, f 0.25: alpha(t) = amplitude
+
+
+def pitching_args(C, cases):
+    """Solver arguments of pitching cases that start from rest at the phase of
+    maximum pitch (istart = 1000): the plates sit at their full amplitude,
+    the hardest phase for the zero-pitch preconditioner."""
+    params, bodies, opts = W.solver_args(cases, C)
+    for p in params:
+        p.istart = MAX_PITCH_STEP
+    return params, bodies, opts
+
+
+def pitch_cg_at_max_amplitude(C, steps=4, amp=30.0):
+    """One config-5 plate at the batch's largest amplitude (30 deg), advanced
+    from rest at the phase of maximum pitch: CG iterations and ms per step of
+    the reference's unpreconditioned CG (cjgr) and of the CG preconditioned by
+    the zero-pitch factor turned with the plate."""
+    out = {}
+    for pre in (0, 1):
+        params, bodies, opts = pitching_args(C, [W.pitching(amp_deg=amp, precond=bool(pre))])
+        g = C.Solver(params[0], bodies[0], opts[0])
+        its, ms = [], []
+        for _ in range(steps):
+            g.advance_n(1, want_hist=False)
+            its.append(g.last_cg_iterations())
+            ms.append(g.last_ms())
+        g.close()
+        out["precond" if pre else "reference_cg"] = {"cg_iterations": its, "ms_per_step": ms}
+    out["workload"] = (f"plate pitching {amp} deg about mid-chord, Re 500, 512x512 cells x 5 levels, dt 0.001, "
+                       "FP64 CG to relative 1e-12, from rest at t = 1 s (alpha = amplitude)")
+    return out
+
+
 def pitching_batch(C, steps=3, warmup=2):
     """Config-5 shape: 32 flat plates pitching about mid-chord with amplitudes
     U[5, 30] deg, Re 500, 512x512 cells x 5 levels, dt 0.001, FP64 CG force
     solve to a relative residual of 1e-12 every step, advanced together."""
     cases = W.pitching_batch(32, seed=SEED)
-    params, bodies, opts = W.solver_args(cases, C)
+    params, bodies, opts = pitching_args(C, cases)
     g = C.Solver(params, bodies, opts)
     g.advance_n(warmup, want_hist=False)
     g.advance_n(steps, want_hist=False)
@@ -289,7 +323,8 @@ def pitching_batch(C, steps=3, warmup=2):
     out = {"value": cells / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
            "cg_iterations_last_step": g.last_cg_iterations(), "kernels_per_step_outside_cg": g.kernels_per_step(),
            "workload": "32 pitching plates (amplitude U[5,30] deg, f 0.25, mid-chord pivot), Re 500, "
-                       "512x512 cells x 5 levels, dt 0.001, FP64 CG to relative residual 1e-12"}
+                       "512x512 cells x 5 levels, dt 0.001, FP64 CG to relative residual 1e-12 preconditioned by "
+                       "the zero-pitch factor, from rest at t = 1 s (maximum pitch)"}
     g.close()
     return out
 
@@ -301,7 +336,7 @@ def pitch_adjoint_cost(C, steps=12, K=6, amp=20.0):
     cost = device time of the gradient run / device time of a plain forward
     run of the same steps from the same state."""
     case = W.pitching(amp_deg=amp)
-    p, b, o = W.solver_args([case], C)
+    p, b, o = pitching_args(C, [case])
     f = C.Solver(p[0], b[0], o[0])
     f.advance_n(steps, want_hist=False)
     ms_plain = f.last_ms()
@@ -316,8 +351,8 @@ def pitch_adjoint_cost(C, steps=12, K=6, amp=20.0):
             "ms_forward_pass": mf, "ms_plain_forward": ms_plain, "steps": steps, "checkpoint_every": K,
             "J": J, "dJ_damp_per_deg": dJ, "adjoint_cg_iterations_max": it,
             "workload": f"plate pitching {amp} deg about mid-chord, f 0.25, Re 500, 512x512 cells x 5 levels, "
-                        f"dt 0.001, FP64 CG to relative 1e-12; J = mean drag over the last {steps // 2} steps, "
-                        "derivative w.r.t. the pitch amplitude"}
+                        f"dt 0.001, preconditioned FP64 CG to relative 1e-12, from rest at t = 1 s; J = mean drag "
+                        f"over the last {steps // 2} steps, derivative w.r.t. the pitch amplitude"}
 
 
 def pitch_adjoint_batch(C, steps=4, K=2):
@@ -328,7 +363,7 @@ def pitch_adjoint_batch(C, steps=4, K=2):
     cost = device time of the gradient run / device time of a plain batched
     forward run of the same steps."""
     cases = W.pitching_batch(32, seed=SEED)
-    params, bodies, opts = W.solver_args(cases, C)
+    params, bodies, opts = pitching_args(C, cases)
     f = C.Solver(params, bodies, opts)
     f.advance_n(steps, want_hist=False)
     ms_plain = f.last_ms()
@@ -344,8 +379,8 @@ def pitch_adjoint_batch(C, steps=4, K=2):
             "adjoint_cg_iterations_max": it, "dJ_damp_per_deg": [float(x) for x in dJ],
             "amp_deg": [c["pitch_amp_deg"] for c in cases],
             "workload": "32 plates pitching U[5,30] deg about mid-chord, f 0.25, Re 500, 512x512 cells x 5 levels, "
-                        f"dt 0.001, FP64 CG to relative 1e-12; J = mean drag over the last {steps // 2} steps; "
-                        "all 32 amplitude derivatives in one batched adjoint run"}
+                        f"dt 0.001, preconditioned FP64 CG to relative 1e-12, from rest at t = 1 s; J = mean drag "
+                        f"over the last {steps // 2} steps; all 32 amplitude derivatives in one batched adjoint run"}
 
 
 def adjoint_cost(C, steps=100, K=50):
@@ -502,6 +537,7 @@ def run_ours(args):
             extras["pitching_batch"] = pitching_batch(C)
             extras["pitch_adjoint"] = pitch_adjoint_cost(C)
             extras["pitch_adjoint_batch"] = pitch_adjoint_batch(C)
+            extras["pitch_cg_at_max_amplitude"] = pitch_cg_at_max_amplitude(C)
             cpu = cpu_sample_from_gpu(g, cases, sorted(int(x) for x in np.random.default_rng(SEED + 2).choice(
                 ncase, 6, replace=False)), args.cpu_steps)
         out = {

@@ -362,8 +362,10 @@ static int adjm_run(ibfs_handle* h, int nsteps, int K, const double* wx, const d
       }
     }
     for (int s = s1 - 1; s >= s0 && rc == IBFS_OK; s--) {
-      // positions, tables, fb and u of step s
+      // preconditioner slot, positions, tables, fb and u of step s
       set_itime(its + s);
+      rc = ensure_precond(h, 0);
+      if (rc) break;
       rc = run_prog(h, M.tables, nullptr);
       if (rc) break;
       const double* after = seg + P.state * (s + 1 - s0);

@@ -563,8 +563,12 @@ static int run_prog(ibfs_handle* h, Prog& P, cudaGraphExec_t ex) {
 // read the per-case active flags between chunks (converged cases skip work
 // inside the CG kernels); returns IBFS_ERR_CG_MAXITER when a case used
 // cg_max_iter iterations (the reference warns and carries on, :435-438).
+static int ensure_precond(ibfs_handle* h, int offset);
+
 static int run_step(ibfs_handle* h) {
-  int rc = run_prog(h, h->prog, h->gexec);
+  int rc = ensure_precond(h, 1);
+  if (rc) return rc;
+  rc = run_prog(h, h->prog, h->gexec);
   if (rc || !h->cg) return rc;
   int maxit = 0;
   for (auto& c : h->cases) maxit = std::max(maxit, c.p.cg_max_iter);
@@ -597,10 +601,10 @@ static int run_step(ibfs_handle* h) {
 }
 
 // ---------------------------------------------------------------------------
-// A case needs the factor of its force operator: stationary bodies for the
-// Cholesky solve, preconditioned CG cases for the preconditioner.
+// A stationary body needs the factor of its force operator for the Cholesky
+// solve (preconditioned CG cases keep their own factors, ensure_precond).
 static bool needs_factor(const HostCase& c) {
-  return (c.p.stationary || c.dc.cg_pre) && !c.have_chol && c.nf > 0;
+  return c.p.stationary && !c.have_chol && c.nf > 0;
 }
 
 // preprocess (operators.f90:29-59) for every case lacking a factor:
@@ -608,25 +612,23 @@ static bool needs_factor(const HostCase& c) {
 // (one per right-hand side, sharing the real case's grid tables, with private
 // scratch), packed from any mix of cases into chunks of a fixed memory budget
 // so that small cases share launches; then one CTA per case factors A.
+static int factor_cases(ibfs_handle* h, const std::vector<int>& need);
+
 static int precompute(ibfs_handle* h) {
   std::vector<int> need;
   for (size_t i = 0; i < h->cases.size(); i++)
     if (needs_factor(h->cases[i])) need.push_back((int)i);
   if (need.empty()) return IBFS_OK;
-  // a preconditioned moving body is factored at its zero-pitch positions:
-  // the regularisation tables are rebuilt there (every step rebuilds its own)
-  std::vector<int> mv;
-  for (int ci : need)
-    if (h->cases[ci].dc.moving) mv.push_back(ci);
-  if (!mv.empty()) {
-    for (int ci : mv) {
-      const DevCase& d = h->cases[ci].dc;
-      IBFS_CUDA_CHECK(cudaMemcpyAsync(d.xb, d.xb0, sizeof(double) * d.nb, cudaMemcpyDeviceToDevice, h->st));
-      IBFS_CUDA_CHECK(cudaMemcpyAsync(d.yb, d.yb0, sizeof(double) * d.nb, cudaMemcpyDeviceToDevice, h->st));
-    }
-    int* dmv = dupload(h, mv);
-    launch_setup_reg_moving(h->d_cases, dmv, (int)mv.size(), h->max_nf, h->max_patch, h->st);
-  }
+  int rc = factor_cases(h, need);
+  if (rc) return rc;
+  for (int ci : need) h->cases[ci].have_chol = true;
+  return IBFS_OK;
+}
+
+// The factor of the force operator of each case in need, with the case's
+// current regularisation tables: columns a_times(e_j) into cholmat, choldc,
+// and the inverse factor into Linv / LinvT.
+static int factor_cases(ibfs_handle* h, const std::vector<int>& need) {
   const size_t budget = (size_t)4 << 30;
   auto per_rhs = [&](const DevCase& c) {
     size_t nsL = (size_t)c.L * c.ns;
@@ -716,7 +718,82 @@ static int precompute(ibfs_handle* h) {
   if (status) return fail(IBFS_ERR_CHOL, "choldc failed");
   launch_chol_inverse(h->d_cases, dcid, nn, h->st);
   IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
-  for (int ci : need) h->cases[ci].have_chol = true;
+  return IBFS_OK;
+}
+
+// Preconditioned CG cases: the slot of the step at device itime + offset
+// (offset 1 before a step, 0 during the adjoint of the step being
+// differentiated), the grid angle nearest the step's pitch; slots not yet
+// factored are factored first, with the body turned by the slot's angle
+// (positions and tables rebuilt there; the step's own move_body restores
+// them). The slot index is a function of the step number alone, so every
+// recomputation of a step uses the same factor.
+#define IBFS_CHECK_OK(x)    \
+  do {                      \
+    int r_ = (x);           \
+    if (r_) return r_;      \
+  } while (0)
+
+static int ensure_precond(ibfs_handle* h, int offset) {
+  std::vector<int> pc;
+  for (size_t i = 0; i < h->cases.size(); i++)
+    if (h->cases[i].dc.cg_pre) pc.push_back((int)i);
+  if (pc.empty()) return IBFS_OK;
+  const int nc = (int)h->cases.size();
+  std::vector<int> it(nc);
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(it.data(), h->d_itime, sizeof(int) * nc, cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  std::vector<int> todo, slot(nc, 0);
+  for (int i : pc) {
+    HostCase& hc = h->cases[i];
+    const DevCase& d = hc.dc;
+    int k = 0;
+    if (d.moving) {
+      double th = -(d.pitch_amp * std::sin(d.pitch_omega * (d.dt * (double)(it[i] + offset))));
+      k = d.pre_k0 + (int)std::lround(th / d.pre_dth);
+      k = std::max(0, std::min(k, (int)hc.pre_done.size() - 1));
+    }
+    slot[i] = k;
+    if (!hc.pre_done[k]) todo.push_back(i);
+  }
+  if (!todo.empty()) {
+    std::vector<int> mv;
+    for (int i : todo) {
+      HostCase& hc = h->cases[i];
+      const DevCase& d = hc.dc;
+      if (!d.moving) continue;
+      // the zero-pitch shape turned by the slot's angle (move_body's rotation)
+      const double th = (double)(slot[i] - d.pre_k0) * d.pre_dth, c = std::cos(th), s = std::sin(th);
+      std::vector<double> x(hc.nb), y(hc.nb);
+      for (int k = 0; k < hc.nb; k++) {
+        double rx = hc.xb[k] - d.pivot_x, ry = hc.yb[k] - d.pivot_y;
+        x[k] = d.pivot_x + c * rx - s * ry;
+        y[k] = d.pivot_y + s * rx + c * ry;
+      }
+      IBFS_CUDA_CHECK(cudaMemcpy(d.xb, x.data(), sizeof(double) * hc.nb, cudaMemcpyHostToDevice));
+      IBFS_CUDA_CHECK(cudaMemcpy(d.yb, y.data(), sizeof(double) * hc.nb, cudaMemcpyHostToDevice));
+      mv.push_back(i);
+    }
+    if (!mv.empty()) {
+      int* dmv = dupload(h, mv);
+      launch_setup_reg_moving(h->d_cases, dmv, (int)mv.size(), h->max_nf, h->max_patch, h->st);
+    }
+    int rc = factor_cases(h, todo);
+    if (rc) return rc;
+    for (int i : todo) {
+      HostCase& hc = h->cases[i];
+      const DevCase& d = hc.dc;
+      size_t nn = (size_t)d.nf * d.nf;
+      double* dst = d.pre_fac + (size_t)slot[i] * 2 * nn;
+      IBFS_CUDA_CHECK(cudaMemcpyAsync(dst, d.Linv, sizeof(double) * nn, cudaMemcpyDeviceToDevice, h->st));
+      IBFS_CUDA_CHECK(cudaMemcpyAsync(dst + nn, d.LinvT, sizeof(double) * nn, cudaMemcpyDeviceToDevice, h->st));
+      hc.pre_done[slot[i]] = 1;
+    }
+  }
+  for (int i : pc)
+    IBFS_CUDA_CHECK(cudaMemcpyAsync(const_cast<int*>(h->cases[i].dc.pre_idx), &slot[i], sizeof(int),
+                                    cudaMemcpyHostToDevice, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));  // slot[] is host stack memory
   return IBFS_OK;
 }
 
@@ -846,6 +923,15 @@ static int setup_case(ibfs_handle* h, HostCase& c, const ibfs_params_c& p, const
     d.cg_y = dalloc<double>(h, c.nf);
     d.cg_sc = dalloc<double>(h, 5);
     d.cg_pre = c.o.cg_precond ? 1 : 0;
+    if (d.cg_pre) {  // factor slots at a 1-degree grid of pitch angles covering the amplitude
+      d.pre_dth = 3.1415926535897932384 / 180.0;
+      d.pre_k0 = d.moving ? (int)std::ceil(std::fabs(d.pitch_amp) / d.pre_dth) : 0;
+      int slots = 2 * d.pre_k0 + 1;
+      d.pre_fac = dalloc<double>(h, (size_t)slots * 2 * c.nf * c.nf, false);
+      d.pre_idx = dalloc<int>(h, 1);
+      c.pre_done.assign(slots, 0);
+      if (!d.pre_fac || !d.pre_idx) return fail(IBFS_ERR_NOMEM, "device allocation failed (preconditioner)");
+    }
     d.cgtol = p.cgtol;
     d.cg_max_iter = p.cg_max_iter;
     d.cg_rel = c.o.cg_relative;
@@ -1297,6 +1383,7 @@ int ibfs_adjoint_pitch_run(ibfs_handle* h, int nsteps, int checkpoint_every, con
 
 int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops) {
   if (!h || !ms || !launches || !flops) return IBFS_ERR_ARG;
+  IBFS_CHECK_OK(ensure_precond(h, 1));
   size_t n = h->prog.size();
   std::vector<cudaEvent_t> ev(n + 1);
   for (auto& e : ev) IBFS_CUDA_CHECK(cudaEventCreate(&e));

@@ -75,7 +75,11 @@ struct DevCase {
   double *cg_r, *cg_d, *cg_q, *cg_q2;  // [Nf]
   double *cg_z, *cg_y;                 // [Nf] preconditioned residual and its half-solve (cg_pre)
   double* cg_sc;                       // delta_new (r.z), delta_old, eps, alpha, r.r
-  int cg_pre;                          // preconditioned by the zero-pitch factor (Linv, LinvT)
+  int cg_pre;                          // preconditioned CG (factors of A at a grid of pitch angles)
+  int pre_k0;                          // slot of zero pitch: slot k = body turned by (k - pre_k0) pre_dth
+  double pre_dth;                      // pitch-angle grid spacing (radians)
+  double* pre_fac;                     // [slots][2][Nf*Nf] Linv, LinvT of each slot (row-major)
+  const int* pre_idx;                  // slot of the step being advanced (set by the host)
   int* cg_it;                          // iterations, active flag
   double cgtol;
   int cg_max_iter, cg_rel;

@@ -27,6 +27,7 @@ struct HostCase {
   std::vector<int> face_ptr, face_f, force_ptr, force_face;
   std::vector<double> face_w, force_w, wsum;
   bool have_chol = false;
+  std::vector<char> pre_done;  // preconditioner slots already factored (cg_precond)
   int out_off = 0;
   int itime = 0;
   DevCase dc{};

@@ -137,18 +137,23 @@ __device__ double block_dot(const double* a, const double* b, int n, double* red
   return r;
 }
 
-// z = P r = Q L0^-T L0^-1 Q^T r (one CTA): the force operator factored at the
-// zero-pitch body, A0 = L0 L0^T (Linv = L0^-1 and LinvT, row-major), applied
-// in the body frame of this step. A rigid rotation by theta moves every
-// point's force pair with it, so A(theta) ~ Q A0 Q^T up to the grid's
-// anisotropy, Q the rotation of each (fx_k, fy_k); theta = 0 for a body that
-// does not move. The triangular products run one warp per row, in a fixed
-// order.
+// z = P r = Q Lk^-T Lk^-1 Q^T r (one CTA): the force operator factored at the
+// body turned by the grid angle theta_k nearest to this step's pitch
+// (A_k = Lk Lk^T; slot k of pre_fac holds Lk^-1 and its transpose, row-major),
+// applied in that slot's frame. A rigid rotation moves every point's force
+// pair with it, so A(theta) ~ Q A_k Q^T up to the grid's anisotropy, Q the
+// rotation by theta - theta_k of each (fx_k, fy_k); theta = 0 for a body that
+// does not move (one slot). The triangular products run one warp per row, in
+// a fixed order.
 __device__ void cg_precond(const DevCase& C, const double* __restrict__ r, double* __restrict__ z) {
   const int nb = C.nb, nf = C.nf;
+  const int slot = *C.pre_idx;
+  const double* __restrict__ Linv = C.pre_fac + (size_t)slot * 2 * nf * nf;
+  const double* __restrict__ LinvT = Linv + (size_t)nf * nf;
   double c = 1.0, s = 0.0;
   if (C.moving) {
     double th = -(C.pitch_amp * sin(C.pitch_omega * (C.dt * (double)(*C.itime))));
+    th = th - (double)(slot - C.pre_k0) * C.pre_dth;
     c = cos(th);
     s = sin(th);
   }
@@ -161,7 +166,7 @@ __device__ void cg_precond(const DevCase& C, const double* __restrict__ r, doubl
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   double* y = C.cg_y;
   for (int row = warp; row < nf; row += nw) {  // y = L0^-1 (Q^T r)
-    const double* Mr = C.Linv + (size_t)row * nf;
+    const double* Mr = Linv + (size_t)row * nf;
     double a = 0.0;
     for (int k = lane; k <= row; k += 32) a = fma(Mr[k], z[k], a);
 #pragma unroll
@@ -170,7 +175,7 @@ __device__ void cg_precond(const DevCase& C, const double* __restrict__ r, doubl
   }
   __syncthreads();
   for (int row = warp; row < nf; row += nw) {  // L0^-T y
-    const double* Mr = C.LinvT + (size_t)row * nf;
+    const double* Mr = LinvT + (size_t)row * nf;
     double a = 0.0;
     for (int k = row + lane; k < nf; k += 32) a = fma(Mr[k], y[k], a);
 #pragma unroll
