@@ -629,12 +629,20 @@ static int precompute(ibfs_handle* h) {
 // current regularisation tables: columns a_times(e_j) into cholmat, choldc,
 // and the inverse factor into Linv / LinvT.
 static int factor_cases(ibfs_handle* h, const std::vector<int>& need) {
-  const size_t budget = (size_t)4 << 30;
   auto per_rhs = [&](const DevCase& c) {
     size_t nsL = (size_t)c.L * c.ns;
     size_t b = sizeof(double) * (2 * nsL + 4 * (size_t)c.ns + c.nq + c.nf);
     return (b + 255) / 256 * 256;
   };
+  // column pool: up to 4 GB, at most half of the free device memory (the
+  // preconditioner slots are factored in the middle of a run), at least one
+  // column of the largest case
+  size_t one = 0;
+  for (int ci : need) one = std::max(one, per_rhs(h->cases[ci].dc));
+  size_t free_b = 0, total_b = 0;
+  size_t budget = (size_t)4 << 30;
+  if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 2);
+  budget = std::max(budget, one);
   char* pool = nullptr;
   if (cudaMalloc(&pool, budget) != cudaSuccess) return fail(IBFS_ERR_NOMEM, "device allocation failed in preprocess");
   struct Rhs { int ci, col; };

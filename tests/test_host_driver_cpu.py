@@ -56,12 +56,12 @@ def test_namelist_reference_style(tmp_path):
 
 def test_options_group_and_geometry(tmp_path):
     write_inp(tmp_path, "&read_parameters m=32, n=32, len=4.0, offsetx=2.0, offsety=2.0, stationary=.true. /\n"
-                        "&B200_OPTIONS PRECISION=1, CG_RELATIVE=T, TILE_CFG=2 /\n")
+                        "&B200_OPTIONS PRECISION=1, CG_RELATIVE=T, TILE_CFG=2, CG_PRECOND=T /\n")
     (tmp_path / "input" / "geom.inp").write_text("3\n 0.1 0.2 0\n -0.25 0.5E-1 0\n 0.3 -0.1 0\n")
     rc, out, err = run(tmp_path)
     assert rc == 0, err
     p = json.loads(out)
-    assert (p["precision"], p["cg_relative"], p["tile_cfg"]) == (1, 1, 2)
+    assert (p["precision"], p["cg_relative"], p["tile_cfg"], p["cg_precond"]) == (1, 1, 2, 1)
     assert (p["nb"], p["x0"], p["y0"]) == (3, 0.1, 0.2)
     # fields not in the file keep the reference defaults (parameters.f90:12-31)
     assert (p["istop"], p["isave"], p["dt"], p["re"], p["mgridlev"]) == (400, 25, 0.005, 300.0, 4)
