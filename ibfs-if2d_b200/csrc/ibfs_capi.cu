@@ -933,14 +933,14 @@ static int setup_case(ibfs_handle* h, HostCase& c, const ibfs_params_c& p, const
     d.cg_pre = c.o.cg_precond ? 1 : 0;
     if (d.cg_pre) {
       // factor slots at a grid of pitch angles covering the amplitude, fine
-      // enough that no body point is more than a quarter cell from where the
-      // nearest slot has it (spacing 0.5 dx / r_max), at most 1 degree and
-      // at most 1025 slots
+      // enough that no body point is more than an eighth of a cell from where
+      // the nearest slot has it (spacing 0.25 dx / r_max), at most 1 degree
+      // and at most 1025 slots
       double rmax = 0.0;
       for (int k = 0; k < nb; k++)
         rmax = std::max(rmax, std::hypot(xb[k] - d.pivot_x, yb[k] - d.pivot_y));
       d.pre_dth = 3.1415926535897932384 / 180.0;
-      if (rmax > 0.0) d.pre_dth = std::min(d.pre_dth, 0.5 * c.delta / rmax);
+      if (rmax > 0.0) d.pre_dth = std::min(d.pre_dth, 0.25 * c.delta / rmax);
       if (d.moving) d.pre_dth = std::max(d.pre_dth, std::fabs(d.pitch_amp) / 512.0);
       d.pre_k0 = d.moving ? (int)std::ceil(std::fabs(d.pitch_amp) / d.pre_dth) : 0;
       int slots = 2 * d.pre_k0 + 1;
