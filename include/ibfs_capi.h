@@ -62,11 +62,13 @@ typedef struct {
   double pitch_amp_deg, pitch_freq, pivot_x, pivot_y;
   int tile_cfg;        /* FP64 transform tile shape 0..3; -1 = the measured autotuner  */
   int cg_precond;      /* CG cases: 0 = cjgr as in the reference (unpreconditioned);
-                          1 = preconditioned CG with the force operator factored at
-                          the zero-pitch body (A0 = L0 L0^T, computed before the first
-                          step like preprocess), applied in the body frame of the step:
-                          z = Q L0^-T L0^-1 Q^T r, Q the pitch rotation of each point's
-                          (fx, fy); same stop rule on the true residual            */
+                          1 = preconditioned CG: the force operator factored with the
+                          body turned by the grid angle nearest the step's pitch
+                          (A_k = L_k L_k^T, one slot per angle of a grid spacing at
+                          most 1 degree, each factored like preprocess on first use),
+                          applied as z = Q L_k^-T L_k^-1 Q^T r with Q the remaining
+                          rotation of each point's (fx, fy); a body that does not move
+                          has one slot. Same stop rule on the true residual        */
 } ibfs_options_c;
 
 typedef struct ibfs_handle ibfs_handle;
