@@ -281,7 +281,7 @@ MAX_PITCH_STEP = 1000  # t = 1/(4 f) = 1 s at dt 0.001, f 0.25: alpha(t) = ampli
 def pitching_args(C, cases):
     """Solver arguments of pitching cases that start from rest at the phase of
     maximum pitch (istart = 1000): the plates sit at their full amplitude,
-    the hardest phase for the zero-pitch preconditioner."""
+    the phase at which the plate has turned farthest."""
     params, bodies, opts = W.solver_args(cases, C)
     for p in params:
         p.istart = MAX_PITCH_STEP
@@ -292,7 +292,8 @@ def pitch_cg_at_max_amplitude(C, steps=4, amp=30.0):
     """One config-5 plate at the batch's largest amplitude (30 deg), advanced
     from rest at the phase of maximum pitch: CG iterations and ms per step of
     the reference's unpreconditioned CG (cjgr) and of the CG preconditioned by
-    the zero-pitch factor turned with the plate."""
+    factors of the force operator at a grid of pitch angles, turned with the
+    plate."""
     out = {}
     for pre in (0, 1):
         params, bodies, opts = pitching_args(C, [W.pitching(amp_deg=amp, precond=bool(pre))])
@@ -324,7 +325,7 @@ def pitching_batch(C, steps=3, warmup=2):
            "cg_iterations_last_step": g.last_cg_iterations(), "kernels_per_step_outside_cg": g.kernels_per_step(),
            "workload": "32 pitching plates (amplitude U[5,30] deg, f 0.25, mid-chord pivot), Re 500, "
                        "512x512 cells x 5 levels, dt 0.001, FP64 CG to relative residual 1e-12 preconditioned by "
-                       "the zero-pitch factor, from rest at t = 1 s (maximum pitch)"}
+                       "factors at a grid of pitch angles, from rest at t = 1 s (maximum pitch)"}
     g.close()
     return out
 

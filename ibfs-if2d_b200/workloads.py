@@ -102,7 +102,7 @@ def pitching(m=512, levels=5, re=500.0, dt=0.001, amp_deg=20.0, freq=0.25, cgtol
     """Flat plate of chord 1 pitching sinusoidally about mid-chord,
     alpha(t) = amp sin(2 pi freq t), body points at spacing dx along the chord;
     the force system is solved by CG to a relative residual of cgtol every step
-    (preconditioned by the zero-pitch factor turned with the plate unless
+    (preconditioned by factors at a grid of pitch angles, turned with the plate, unless
     precond is False)."""
     c = case(m, levels, re, dt, "plate", aoa=0.0)
     c.update(pitch_amp_deg=float(amp_deg), pitch_freq=float(freq), cgtol=float(cgtol), cg_precond=int(bool(precond)))

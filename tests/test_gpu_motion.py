@@ -132,7 +132,7 @@ def test_amplitude_derivative_by_central_differences():
 
 
 def test_preconditioned_cg_matches_plain_cg():
-    """cg_precond = 1: CG preconditioned by the zero-pitch factor turned with
+    """cg_precond = 1: CG preconditioned by factors at a grid of pitch angles turned with
     the plate reaches the same relative 1e-12 solution as the reference's
     unpreconditioned cjgr (forces within 1e-10) in fewer iterations; on a
     body that does not move it is the inverse of A's symmetric part (A is
