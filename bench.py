@@ -280,8 +280,8 @@ MAX_PITCH_STEP = 1000  # t = 1/(4 f) = 1 s at dt 0.001, f 0.25: alpha(t) = ampli
 
 def pitching_args(C, cases):
     """Solver arguments of pitching cases that start from rest at the phase of
-    maximum pitch (istart = 1000): the plates sit at their full amplitude,
-    the phase at which the plate has turned farthest."""
+    maximum pitch (istart = 1000), where the plates sit at their full
+    amplitude and the CG force solve needs the most iterations."""
     params, bodies, opts = W.solver_args(cases, C)
     for p in params:
         p.istart = MAX_PITCH_STEP
