@@ -265,13 +265,24 @@ def plain_and_split_plate(C, torch, steps, warmup, flush):
     cd = np.abs(fx0).max()
     L = nlev_plate
     om0, om1 = s0["omega"].reshape(L, -1), s1["omega"].reshape(L, -1)  # omega(2:m,2:n,L), level slowest
-    per_level = [float(np.abs(om1[k] - om0[k]).max() / np.abs(om0[k]).max()) for k in range(L)]
+    q0_, q1_ = s0["q"].reshape(L, -1), s1["q"].reshape(L, -1)
+
+    def rel_max(a, b):
+        return float(np.abs(a - b).max() / np.abs(b).max())
+
+    def rel_l2(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    per_level = [rel_max(om1[k], om0[k]) for k in range(L)]
+    field_err = {"omega_rel_l2_per_level": [rel_l2(om1[k], om0[k]) for k in range(L)],
+                 "q_rel_max_per_level": [rel_max(q1_[k], q0_[k]) for k in range(L)],
+                 "q_rel_l2_per_level": [rel_l2(q1_[k], q0_[k]) for k in range(L)]}
     plain = dict(out[0], workload=PLATE["workload"], form="plain FP64",
                  l2="flushed between timed steps (256 MB write)")
     split = dict(out[1], workload=PLATE["workload"], form="split-precision (single case)",
                  err_vs_fp64={"steps": 40, "cd_rel_max": float(np.abs(fx1 - fx0).max() / cd),
                               "cl_rel_to_max_cd": float(np.abs(fy1 - fy0).max() / cd),
-                              "omega_rel_max_per_level": per_level})
+                              "omega_rel_max_per_level": per_level, **field_err})
     return plain, split
 
 
