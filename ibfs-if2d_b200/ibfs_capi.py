@@ -257,6 +257,9 @@ class Solver:
         bv = None if body_vel is None else np.ascontiguousarray(body_vel, dtype=np.float64)
         wx = np.ascontiguousarray(wx, dtype=np.float64)
         wy = np.ascontiguousarray(wy, dtype=np.float64)
+        need = nsteps * self.sizes[0]["nbody"]
+        if wx.size != need or wy.size != need:
+            raise ValueError(f"wx and wy need {need} weights (nsteps x nbody), got {wx.size} and {wy.size}")
         J, ms_f, ms_t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         grad = np.zeros(nf)
         self._check(lib().ibfs_adjoint_run(self.h, nsteps, checkpoint_every, _p(bv), _p(wx), _p(wy),
@@ -286,6 +289,10 @@ class Solver:
         if wx.ndim == 1 and nc > 1:
             wx, wy = np.tile(wx, nc), np.tile(wy, nc)
         wx, wy = np.ascontiguousarray(wx.ravel()), np.ascontiguousarray(wy.ravel())
+        need = nsteps * sum(sz["nbody"] for sz in self.sizes)
+        if wx.size != need or wy.size != need:
+            raise ValueError(f"wx and wy need {need} weights (nsteps x nbody per case, case-major), "
+                             f"got {wx.size} and {wy.size}")
         J, dJ = np.zeros(nc), np.zeros(nc)
         ms_f, ms_t = ctypes.c_double(), ctypes.c_double()
         self._check(lib().ibfs_adjoint_pitch_run(self.h, nsteps, checkpoint_every, _p(wx), _p(wy), _p(J), _p(dJ),

@@ -62,3 +62,20 @@ def test_error_statuses_without_gpu(so_path):
     assert rc == 7
     assert L.ibfs_advance_n(None, 1, None) == 7
     assert L.ibfs_batch_advance(None, None, None) == 7
+
+
+def test_adjoint_weight_lengths_checked():
+    """The adjoint wrappers refuse objective weights that do not cover
+    nsteps x nbody per case (the C side would read past them); the check
+    runs before any library call, so a handle-less Solver shows it."""
+    import ibfs_capi as C
+    s = C.Solver.__new__(C.Solver)
+    s.h, s.ncases = None, 2
+    s.sizes = [dict(nbody=1, nf=10), dict(nbody=2, nf=10)]
+    with pytest.raises(ValueError):
+        s.adjoint_pitch_run(4, 2, np.zeros(4), np.zeros(4))  # tiled 1-D: 8 weights, 12 needed
+    with pytest.raises(ValueError):
+        s.adjoint_pitch_run(4, 2, np.zeros(11), np.zeros(11))
+    s.ncases, s.sizes = 1, [dict(nbody=3, nf=10)]
+    with pytest.raises(ValueError):
+        s.adjoint_run(4, 2, None, np.zeros(4), np.zeros(4))
