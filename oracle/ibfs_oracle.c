@@ -710,6 +710,8 @@ static double dot(const double* a, const double* b, int n) {
 /* cjgr (operators.f90:393-441): x holds the initial guess on entry. */
 static int cjgr(or_case* c, double* x, const double* b, int* iters) {
   int nf = c->nf;
+  if (iters) *iters = 0;
+  if (nf <= 0) return 0;  /* no body points: nothing to solve */
   double* r = (double*)malloc(sizeof(double) * nf);
   double* d = (double*)malloc(sizeof(double) * nf);
   double* q = (double*)malloc(sizeof(double) * nf);
