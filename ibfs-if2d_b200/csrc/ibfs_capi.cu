@@ -404,7 +404,7 @@ static void build_step_program(ibfs_handle* h) {
   std::vector<int> ids;
   for (size_t i = 0; i < h->cases.size(); i++) { cs.push_back(h->cases[i].dc); ids.push_back((int)i); }
   int nc = (int)cs.size();
-  int Lmax = h->max_L, mns = h->max_ns, mnf = h->max_nf, mring = h->max_ring;
+  int Lmax = h->max_L, mnf = h->max_nf, mring = h->max_ring;
   const int* d_ids = B.ints(ids);
   B.add([=]() { launch_step_begin(dcases, nc, st); });
   // move_body + setup_reg for moving bodies (operators.f90:142-144); step 1
@@ -1473,10 +1473,10 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
   std::vector<int> ids{0};
   const int* dids = B.ints(ids);
   int rc = IBFS_OK;
-  size_t in_n = 0, out_n = 0;
+  size_t out_n = 0;
   double* dout = nullptr;
   if (op == 0 || op == 1 || op == 2) {
-    in_n = ns; out_n = ns;
+    out_n = ns;
     IBFS_CUDA_CHECK(cudaMemcpy(s.vort, in, ns * sizeof(double), cudaMemcpyHostToDevice));
     if (h->precision == 1) {
       rc = precision_apply_op(h->prec, op, ds, s, st);
@@ -1495,7 +1495,7 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
       dout = s.omega;
     }
   } else if (op == 3) {  // a_times
-    in_n = c.nf; out_n = c.nf;
+    out_n = c.nf;
     IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
     IBFS_CUDA_CHECK(cudaMemset(s.omega, 0, (size_t)c.L * ns * sizeof(double)));
     auto bm1 = B.bmap({(int)ns});
@@ -1511,7 +1511,7 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
     B.add([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
     dout = s.wc;
   } else if (op == 4) {  // regT
-    in_n = c.nq; out_n = c.nf;
+    out_n = c.nf;
     IBFS_CUDA_CHECK(cudaMemcpy(s.q, in, c.nq * sizeof(double), cudaMemcpyHostToDevice));
     std::vector<double*> o1{s.wc};
     double** douts = dupload(&tmp, o1);
@@ -1519,7 +1519,7 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
     B.add([=]() { launch_regT_out(ds, dids, 1, nf, douts, st); });
     dout = s.wc;
   } else if (op == 5) {  // rot(reg(f))
-    in_n = c.nf; out_n = ns;
+    out_n = ns;
     IBFS_CUDA_CHECK(cudaMemcpy(s.fb, in, c.nf * sizeof(double), cudaMemcpyHostToDevice));
     auto bm1 = B.bmap({(int)ns});
     B.add([=]() { launch_regrot(ds, dids, bm1.first, bm1.second, st); });
@@ -1527,7 +1527,6 @@ static int run_apply_op(ibfs_handle* h, int op, const double* in, double* out) {
   } else {
     rc = fail(IBFS_ERR_ARG, "unknown op");
   }
-  (void)in_n;
   if (rc == IBFS_OK) {
     for (auto& f : P) f.fn();
     cudaError_t e = cudaStreamSynchronize(st);
