@@ -79,3 +79,19 @@ def test_adjoint_weight_lengths_checked():
     s.ncases, s.sizes = 1, [dict(nbody=3, nf=10)]
     with pytest.raises(ValueError):
         s.adjoint_run(4, 2, None, np.zeros(4), np.zeros(4))
+
+
+def test_pitching_workload_options():
+    """workloads.solver_args turns pitching cases into moving-body CG options
+    (relative stop, device pitching, preconditioned unless asked otherwise)
+    and stationary cases into Cholesky ones."""
+    import ibfs_capi as C
+    import workloads as W
+    cases = [W.pitching(m=64, levels=3, amp_deg=12.5), W.pitching(m=64, levels=3, amp_deg=7.0, precond=False),
+             W.case(64, 3, 100.0, 0.01, "cylinder")]
+    params, bodies, opts = W.solver_args(cases, C)
+    assert [p.stationary for p in params] == [0, 0, 1]
+    assert [o.motion_kind for o in opts] == [1, 1, 0]
+    assert [o.cg_precond for o in opts] == [1, 0, 0]
+    assert opts[0].cg_relative == 1 and opts[0].pitch_amp_deg == 12.5 and opts[0].pitch_freq == 0.25
+    assert params[0].cgtol == 1e-12 and len(bodies[0][0]) == int(1.0 / (4.0 / 64)) + 1
