@@ -157,3 +157,25 @@ def test_cg_maxiter_reports(oracle_mod):
     b = O.Case(O.make_params(m, m, 0.01, 100.0, 3, stationary=False, cgtol=1e-30, cg_max_iter=2), xb, yb)
     rc, o = b.advance()
     assert rc == 3 and o["cg_iters"] == 2
+
+
+def test_cn_update_identity(case32):
+    """The Crank-Nicolson/AB2 level update as the reference evaluates it with
+    its spectral tables (operators.f90:126-130, tables myfft.f90:46-69),
+    w = dst(lam1i (dst(con1 rhs + con2 rold) + lam1 dst(omega))), solves
+    (I + nu C^T C) w = (I - nu C^T C) omega + 1.5 dt/d^2 rhs - 0.5 dt/d^2 rold
+    on every level (d = delta 2^(k-1), nu = dt / (2 Re d^2); no boundary terms)."""
+    c = case32
+    t = c.tables()
+    rng = np.random.default_rng(7)
+    dt, re = c.params.dt, c.params.re
+    for k in range(c.nlev):
+        lam1 = t["lam1"][k * c.ns:(k + 1) * c.ns]
+        lam1i = t["lam1i"][k * c.ns:(k + 1) * c.ns]
+        om, rhs, rold = (rng.standard_normal(c.ns) for _ in range(3))
+        w = c.dst(lam1i * (c.dst(t["con1"][k] * rhs + t["con2"][k] * rold) + lam1 * c.dst(om)))
+        d2 = (c.delta * 2.0 ** k) ** 2
+        nu = 0.5 * dt / (re * d2)
+        lhs = w + nu * laplacian(c, w)
+        rhs_ = om - nu * laplacian(c, om) + 1.5 * dt / d2 * rhs - 0.5 * dt / d2 * rold
+        assert rel(lhs, rhs_) < 1e-12, k
