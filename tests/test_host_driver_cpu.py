@@ -165,3 +165,24 @@ def test_actuator_slots(tmp_path):
     (tmp_path / "input" / "slot.002.inp").unlink()
     rc, out, err = run(tmp_path)
     assert rc != 0 and "slot.002.inp" in err
+
+
+def test_actuator_slots_after_spec_primitives(tmp_path):
+    """Primitives from input/geom.spec, then the actuators' slot points after
+    them (grid.f90:382-401: the primitives, then each actuator_slot)."""
+    import oracle as O
+    m = 64
+    ds = 4.0 / m
+    write_inp(tmp_path, f"&READ_PARAMETERS M = {m}, N = {m}, LEN = 4.0, OFFSETX = 2, OFFSETY = 2 /\n")
+    (tmp_path / "input" / "geom.spec").write_text("circle 1.0 0.0 0.0 0\n")
+    (tmp_path / "input" / "actuator.001.inp").write_text(
+        " &READ_ACT_PARAMETERS X_J = 0.6, Y_J = 0.0, H_J = 0.25, U_J = 1.0, U_J_OSC = 0.0, "
+        "THETA_J = 0.0, OMG_J = 0.0 /\n")
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    p = json.loads(out)
+    ncirc = int(np.pi * 1.0 / ds)
+    ax, ay, _ = O.actuator_slot(0.6, 0.0, 0.25, ds, 0.0, -1)
+    assert (p["n_act"], p["n_act_pt"], p["nb"]) == (1, len(ax), ncirc + len(ax))
+    xc, yc = O.circle(ds, 1.0, 0.0, 0.0)
+    assert abs(p["xsum"] - (xc.sum() + ax.sum())) <= 1e-13 and abs(p["ysum"] - (yc.sum() + ay.sum())) <= 1e-13
