@@ -2,11 +2,10 @@
 //
 // Some callers cannot call cudaMalloc at the point where they need a
 // transform: a driver that hands every byte of device memory to its own pool
-// manager up front, code that runs while a stream is being captured into a
-// CUDA graph (allocation is not allowed there), or a host language runtime
-// that forbids the CUDA allocator on its solver thread. ibfs_dst2d_noalloc
-// serves them. The caller passes device pointers to the input and output
-// fields; the intermediate product of the two transform halves lives in the
+// manager up front, or a host language runtime that forbids the CUDA
+// allocator on its solver thread. ibfs_dst2d_noalloc serves them. The
+// caller passes device pointers to the input and output fields; the
+// intermediate product of the two transform halves lives in the
 // file-scope array below, and the sine coefficients are computed in the
 // kernels, so no descriptor, table or work buffer is allocated.
 //
@@ -96,7 +95,9 @@ static double* g_noalloc_ptr[kMaxDevices] = {nullptr};
 
 // Device address of the scratch array for the current device. The array's
 // name is only a host-side stand-in in host code, so the address is looked up
-// once per device with that device current, on the first call there.
+// once per device with that device current, on the first call there. The
+// address is the one in the device's primary context (the CUDA runtime's);
+// it is kept for the life of the process.
 static int noalloc_scratch(double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -123,6 +124,12 @@ extern "C" int ibfs_dst2d_noalloc(const double* d_in, double* d_out, int m, int 
   if (m < 2 || n < 2 || m - 1 > kNoAllocMaxN || n - 1 > kNoAllocMaxN)
     return set_error(IBFS_ERR_ARG,
                      "ibfs_dst2d_noalloc: m-1 and n-1 must be in [1, 511] (grids up to 512x512 cells)");
+  // An error left pending by earlier work on this thread stays the caller's:
+  // refuse to launch rather than clear it and report it as this call's own.
+  cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return set_error(IBFS_ERR_CUDA, (std::string("ibfs_dst2d_noalloc: an earlier CUDA error is pending: ") +
+                                     cudaGetErrorString(pending)).c_str());
   double* scratch = nullptr;
   int rc = noalloc_scratch(&scratch);
   if (rc) return rc;

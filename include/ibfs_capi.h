@@ -235,9 +235,8 @@ int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops);
 /* 2-D DST-I (the reference's dst, myfft.f90:83-94) of a device field that
  * allocates no device memory. No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc where they need a transform -- a driver
- * whose memory pool owns all device memory, code running inside CUDA-graph
- * stream capture, or a runtime that keeps the CUDA allocator off its solver
- * thread. d_in, d_out: device pointers to (m-1)*(n-1) doubles in the Fortran
+ * whose memory pool owns all device memory, or a runtime that keeps the CUDA
+ * allocator off its solver thread. d_in, d_out: device pointers to (m-1)*(n-1) doubles in the Fortran
  * node layout; stream: a cudaStream_t (NULL = default stream); the call is
  * asynchronous on it. Limit: m-1, n-1 <= 511 (grids up to 512x512 cells),
  * else IBFS_ERR_ARG. The intermediate product lives in one file-scope device
@@ -245,8 +244,26 @@ int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops);
  * until exit), shared by all calls: calls that overlap on the GPU race and
  * must be serialised by the caller. The first call on a device looks up that
  * array's device address (with that device current); make the first call
- * before any stream capture. Errors: ibfs_last_error(NULL). */
+ * before any stream capture. That address belongs to the device's primary
+ * context (the CUDA runtime's) and is kept for the life of the process; it is
+ * not looked up again after cudaDeviceReset. A CUDA error already pending on
+ * the calling thread is left in place and the call returns IBFS_ERR_CUDA
+ * without launching. Errors: ibfs_last_error(NULL). */
 int ibfs_dst2d_noalloc(const double* d_in, double* d_out, int m, int n, void* stream);
+
+/* Limit of every bounded device wait of the handle, in seconds (0..60; the
+ * default is 1). The only device-side waits are the mbarrier waits of the
+ * split-precision form's tensor-core GEMM; on a plain FP64 handle the call
+ * has no effect. A wait that passes the limit makes its thread block stop
+ * work, wait for its own copies and products still in flight, free its
+ * tensor memory and return; the advance then returns IBFS_ERR_TIMEOUT with
+ * the role, block and pipeline step of the first wait that gave up, and the
+ * handle's state is undefined (destroy it). A limit of 0 makes every wait
+ * that does not succeed at once give up: it exercises this path (the
+ * reference's counterpart is none; its waits cannot time out). The value is
+ * read by the kernel from device memory, so it applies to captured step
+ * graphs too. */
+int ibfs_set_wait_limit(ibfs_handle* h, double seconds);
 
 /* Message of the last error on this handle (or of the last failed create). */
 const char* ibfs_last_error(const ibfs_handle* h);

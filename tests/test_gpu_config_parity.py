@@ -1,0 +1,160 @@
+"""GPU parity with the CPU oracle at the benchmark configurations' sizes.
+
+Every GPU call goes through the C-ABI; the oracle (oracle/ibfs_oracle.c) runs
+the same case from the same inputs in a spawn-started process pool (all jobs
+submitted when the first test of this file runs, so they overlap).
+
+Cases:
+  * the stationary cylinder configuration exactly: D=1, 126 points, 200x200
+    cells, 3 levels, Re 100, dt 0.004, 50 steps;
+  * the flat plate configuration's grid: chord 1 at 30 deg, Re 300, 400x400
+    cells, 5 levels, dt 0.002, 10 steps, plain and split precision;
+  * a 5-level cylinder on 128x128 cells, 30 steps, both forms;
+  * one batch holding one case of every grid size of the batched workload
+    (128, 192, 256, 384, 512) and every level count 2..5, both forms;
+  * the split form over 400 steps of a 128x128x3 plate.
+
+Bars: the plain FP64 method within 1e-10, the split-precision form within
+1e-8, on
+  - omega, rhs_old and q per level: max |error| / max |oracle value| of that
+    level (the split form also reports relative L2 per level);
+  - fb: max |error| / max |fb|;
+  - drag and lift per step: max(|dCd|, |dCl|) / |(Cd, Cl)| of that step;
+  - circulation per level per step (write_circ, operators.f90:662-699):
+    |d circ_k| / sum |omega_k|. A symmetric cylinder's circulation is a sum
+    of terms that cancel to round-off (~1e-15), so it is compared against the
+    sum of the magnitudes that it adds up, the condition number of that sum;
+  - slip per step (write_slip, operators.f90:549-580): |d slip| / max
+    |regT(q0)|. Slip is the residual of the no-slip constraint, a difference
+    of body-point velocities of size max |regT(q0)| that cancel to ~1e-8, so
+    it is compared against the size of the terms it is a difference of.
+"""
+import numpy as np
+import pytest
+
+import ibfs_capi as C
+import oracle_runs as R
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_TOL = 1e-10
+SPLIT_TOL = 1e-8
+
+CYL200 = W.cylinder_re100()
+PLATE400 = W.plate_re300()
+CYL128_L5 = W.case(128, 5, 100.0, 0.004, "cylinder")
+PLATE128_LONG = W.case(128, 3, 300.0, 0.4 * 4.0 / 128, "plate", aoa=30.0)
+# one case of each grid size of the batched workload and each level count 2..5
+MIX = [W.case(128, 5, 80.0, 0.4 * 4.0 / 128, "cylinder"),
+       W.case(192, 2, 300.0, 0.4 * 4.0 / 192, "plate", aoa=20.0),
+       W.case(256, 3, 150.0, 0.4 * 4.0 / 256, "cylinder"),
+       W.case(384, 4, 60.0, 0.4 * 4.0 / 384, "plate", aoa=35.0),
+       W.case(512, 5, 450.0, 0.4 * 4.0 / 512, "plate", aoa=10.0)]
+STEPS = {"cyl200": 50, "plate400": 10, "cyl128_l5": 30, "mix": 8, "plate128_long": 400}
+
+
+@pytest.fixture(scope="module")
+def pool():
+    p = R.Pool()
+    p.submit("plate400", R.run_case, PLATE400, STEPS["plate400"])
+    for i, c in enumerate(MIX):
+        p.submit(f"mix{i}", R.run_case, c, STEPS["mix"])
+    p.submit("cyl200", R.run_case, CYL200, STEPS["cyl200"])
+    p.submit("cyl128_l5", R.run_case, CYL128_L5, STEPS["cyl128_l5"])
+    p.submit("plate128_long", R.run_case, PLATE128_LONG, STEPS["plate128_long"])
+    yield p
+    p.close()
+
+
+def rel_max(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def compare(g, hist, ic, ref, tol):
+    """Errors of case ic of handle g (history hist from advance_n) against an
+    oracle run; asserts each against tol and returns them."""
+    L = ref["nlev"]
+    sg, so = g.get_state(ic), ref["state"]
+    errs = {}
+    for k in ("omega", "rhs_old", "q"):
+        a, b = sg[k].reshape(L, -1), so[k].reshape(L, -1)
+        errs[k] = [rel_max(a[l], b[l]) for l in range(L)]
+        errs[k + "_l2"] = [rel_l2(a[l], b[l]) for l in range(L)]
+    errs["fb"] = rel_max(sg["fb"], so["fb"])
+    steps = hist.shape[0]
+    out = [g.outputs_of(hist[s], ic) for s in range(steps)]
+    fx = np.array([o["fx"] for o in out])
+    fy = np.array([o["fy"] for o in out])
+    circ = np.array([o["circ"] for o in out])
+    slip = np.array([o["slip"] for o in out])
+    fmag = np.sqrt(ref["fx"] ** 2 + ref["fy"] ** 2)
+    errs["force"] = float(np.max(np.maximum(np.abs(fx - ref["fx"]), np.abs(fy - ref["fy"])) / fmag))
+    l1 = np.abs(so["omega"].reshape(L, -1)).sum(axis=1)
+    errs["circ"] = float(np.max(np.abs(circ - ref["circ"]) / l1[None, :]))
+    errs["slip"] = float(np.max(np.abs(slip - ref["slip"])) / ref["slip_scale"])
+    for k in ("omega", "rhs_old", "q"):
+        assert max(errs[k]) < tol, (k, errs[k])
+    for k in ("fb", "force", "circ", "slip"):
+        assert errs[k] < tol, (k, errs[k])
+    return errs
+
+
+def single(case, precision, steps):
+    params, bodies, opts = W.solver_args([case], C, precision)
+    g = C.Solver(params[0], bodies[0], opts[0])
+    hist = g.advance_n(steps)
+    return g, hist
+
+
+def test_cylinder_config_plain(pool):
+    """The stationary cylinder configuration, 50 steps, plain FP64."""
+    g, hist = single(CYL200, 0, STEPS["cyl200"])
+    assert g.sizes[0]["nb"] == 126 and g.sizes[0]["nlev"] == 3
+    e = compare(g, hist, 0, pool.get("cyl200"), PLAIN_TOL)
+    print("cylinder 200x200x3:", e)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, PLAIN_TOL), (1, SPLIT_TOL)])
+def test_plate_config_five_levels(pool, precision, tol):
+    """The flat-plate configuration's 400x400x5 grid: plain FP64 at 1e-10, and
+    the split-precision form against the FP64 oracle per field and per force
+    coefficient at 1e-8."""
+    g, hist = single(PLATE400, precision, STEPS["plate400"])
+    assert g.sizes[0]["nlev"] == 5
+    e = compare(g, hist, 0, pool.get("plate400"), tol)
+    print(f"plate 400x400x5 precision={precision}:", e)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, PLAIN_TOL), (1, SPLIT_TOL)])
+def test_five_level_cylinder_128(pool, precision, tol):
+    g, hist = single(CYL128_L5, precision, STEPS["cyl128_l5"])
+    assert g.sizes[0]["nlev"] == 5
+    compare(g, hist, 0, pool.get("cyl128_l5"), tol)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, PLAIN_TOL), (1, SPLIT_TOL)])
+def test_batch_every_size_and_level_count(pool, precision, tol):
+    """One handle advancing a case of every grid size (128..512) and level
+    count (2..5) of the batched workload together, each case against its own
+    oracle run."""
+    params, bodies, opts = W.solver_args(MIX, C, precision)
+    g = C.Solver(params, bodies, opts)
+    assert sorted({s["nlev"] for s in g.sizes}) == [2, 3, 4, 5]
+    hist = g.advance_n(STEPS["mix"])
+    for i in range(len(MIX)):
+        e = compare(g, hist, i, pool.get(f"mix{i}"), tol)
+        print(f"mix case {i} m={MIX[i]['m']} L={MIX[i]['levels']} precision={precision}: "
+              f"omega {max(e['omega']):.2e} force {e['force']:.2e}")
+
+
+def test_split_form_long_horizon(pool):
+    """The split-precision form stays within 1e-8 of the FP64 oracle over 400
+    steps (drag and lift at every step, fields at the end)."""
+    g, hist = single(PLATE128_LONG, 1, STEPS["plate128_long"])
+    e = compare(g, hist, 0, pool.get("plate128_long"), SPLIT_TOL)
+    print("split form, 128x128x3 plate, 400 steps:", e)

@@ -1,12 +1,12 @@
 """The allocation-free 2-D DST entry point (ibfs_dst2d_noalloc) against the
-existing handle-based one (ibfs_apply_op, op 0).
+existing handle-based transform (ibfs_apply_op, op 0) and against the
+oracle's dst.
 
 ibfs_dst2d_noalloc is for callers that cannot call cudaMalloc where they need
-the transform (a memory pool that owns all device memory, code running under
-CUDA-graph stream capture, a runtime that keeps the CUDA allocator off its
-solver thread): its intermediate product lives in a fixed file-scope device
-array and it takes device pointers the caller already owns. This file is
-named so that pytest collects it last.
+the transform: a driver whose memory pool owns all device memory, or a runtime
+that keeps the CUDA allocator off its solver thread. Its intermediate product
+lives in a fixed file-scope device array and it takes device pointers that the
+caller already owns. This file is named so that pytest collects it last.
 """
 import ctypes
 
@@ -26,10 +26,11 @@ def _noalloc(x_dev, y_dev, m, n, stream):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("m,n", [(64, 48), (400, 400), (512, 512)])
-def test_noalloc_dst_matches_handle_dst(m, n):
+def test_noalloc_dst_matches_handle_dst_and_oracle(m, n):
     import torch
     xb, yb = O.circle(4.0 / m, 1.0, 0.0, 0.0)
     g = C.Solver(C.make_params(m, n, 0.01, 100.0, 2), (xb, yb))
+    oc = O.Case(O.make_params(m, n, 0.01, 100.0, 2), xb, yb)
     rng = np.random.default_rng(11)
     ns = (m - 1) * (n - 1)
     stream = torch.cuda.current_stream().cuda_stream
@@ -44,6 +45,9 @@ def test_noalloc_dst_matches_handle_dst(m, n):
         y = y_dev.cpu().numpy()
         err = np.abs(y - ref).max() / np.abs(ref).max()
         assert err < TOL, (call, err)
+        orc = oc.dst(x)
+        err_o = np.abs(y - orc).max() / np.abs(orc).max()
+        assert err_o < TOL, (call, err_o)
     g.close()
 
 
