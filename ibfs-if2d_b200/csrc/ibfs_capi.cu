@@ -1113,6 +1113,24 @@ static void free_adj(ibfs_handle* h) {
 
 // ===========================================================================
 // C-ABI
+// Status word of the tensor-core GEMM after a step: bit 2 = a bounded wait
+// gave up (status[1..3]: role, block, pipeline step of the first one), bit 4 =
+// a drain wait gave up as well. Reads it with the stream synchronised.
+static int check_device_waits(ibfs_handle* h) {
+  int st4[4] = {0, 0, 0, 0};
+  IBFS_CUDA_CHECK(cudaMemcpyAsync(st4, h->d_status, sizeof(st4), cudaMemcpyDeviceToHost, h->st));
+  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  if (!(st4[0] & 2)) return IBFS_OK;
+  static const char* roles[] = {"?", "producer waiting for a free stage", "MMA waiting for a free accumulator",
+                                "MMA waiting for a loaded stage", "epilogue waiting for an accumulator"};
+  const int r = (st4[1] >= 1 && st4[1] <= 4) ? st4[1] : 0;
+  std::string msg = std::string("a bounded device wait gave up (tensor-core GEMM: ") + roles[r] + ", block " +
+                    std::to_string(st4[2]) + ", step " + std::to_string(st4[3]) + ")";
+  if (st4[0] & 4) msg += "; a drain of in-flight copies also gave up";
+  msg += "; the handle's state is undefined";
+  return fail(IBFS_ERR_TIMEOUT, msg);
+}
+
 extern "C" {
 
 int ibfs_batch_create(int ncases, const ibfs_params_c* p, const ibfs_options_c* opt, const int* nb,
@@ -1267,6 +1285,10 @@ int ibfs_advance(ibfs_handle* h, int* itime, const double* body_vel, double* fx,
   double* o = h->h_stage + c.nf;
   IBFS_CUDA_CHECK(cudaMemcpyAsync(o, h->d_out, sizeof(double) * h->out_stride, cudaMemcpyDeviceToHost, h->st));
   IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
+  {
+    int wrc = check_device_waits(h);
+    if (wrc) { h->err = t_error; return wrc; }
+  }
   *itime += 1;
   c.itime = *itime;
   if (fx) memcpy(fx, o, sizeof(double) * c.nbody);
@@ -1294,10 +1316,10 @@ int ibfs_batch_advance(ibfs_handle* h, const double* body_vel, double* out) {
   if (rc && rc != IBFS_ERR_CG_MAXITER) { h->err = t_error; return rc; }
   if (rc) h->err = t_error;
   IBFS_CUDA_CHECK(cudaMemcpyAsync(h->h_stage, h->d_out, sizeof(double) * h->out_stride, cudaMemcpyDeviceToHost, h->st));
-  int status = 0;
-  IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-  IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
-  if (status & 2) return fail(IBFS_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM)");
+  {
+    int wrc = check_device_waits(h);
+    if (wrc) { h->err = t_error; return wrc; }
+  }
   if (out) memcpy(out, h->h_stage, sizeof(double) * h->out_stride);
   for (auto& c : h->cases) c.itime += 1;
   return rc;
@@ -1331,11 +1353,12 @@ int ibfs_advance_n(ibfs_handle* h, int nsteps, double* hist) {
   if (hist)
     IBFS_CUDA_CHECK(cudaMemcpyAsync(hist, h->d_hist, sizeof(double) * (size_t)nsteps * h->out_stride,
                                     cudaMemcpyDeviceToHost, h->st));
-  int status = 0;
-  IBFS_CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
   IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
   cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
-  if (status & 2) return fail(IBFS_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM)");
+  {
+    int wrc = check_device_waits(h);
+    if (wrc) { h->err = t_error; return wrc; }
+  }
   for (auto& c : h->cases) c.itime += nsteps;
   return warn;
 }
@@ -1422,6 +1445,17 @@ int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops) 
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (auto& c : h->cases) c.itime += 1;
+  int wrc = check_device_waits(h);
+  if (wrc) h->err = t_error;
+  return wrc;
+}
+
+int ibfs_set_wait_limit(ibfs_handle* h, double seconds) {
+  if (!h || !(seconds >= 0.0) || seconds > 60.0)
+    return fail(IBFS_ERR_ARG, "ibfs_set_wait_limit: seconds must be in [0, 60]");
+  if (!h->prec) return IBFS_OK;  // plain FP64 handles have no bounded device waits
+  int rc = precision_set_wait_limit(h->prec, seconds);
+  if (rc) return fail(rc, "ibfs_set_wait_limit: cannot write the limit to the device");
   return IBFS_OK;
 }
 

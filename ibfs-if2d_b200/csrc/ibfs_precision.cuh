@@ -17,6 +17,8 @@ using Alloc = std::function<void*(size_t)>;
 int precision_init(PrecisionPlan*& pp, cudaStream_t st, const std::vector<DevCase>& cases, const DevCase* d_cases,
                    Alloc alloc);
 void precision_free(PrecisionPlan* pp);
+// Limit (seconds, 0..60) of every bounded wait of the tensor-core GEMM.
+int precision_set_wait_limit(PrecisionPlan* pp, double seconds);
 const char* precision_error();
 void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, const std::vector<DevCase>& cs,
                            cudaStream_t st);

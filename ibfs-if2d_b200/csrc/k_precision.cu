@@ -59,12 +59,18 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Every wait gives up after this long (a healthy wait lasts microseconds).
+// Default limit of every wait (a healthy wait lasts microseconds); the
+// handle keeps the limit in device memory (ibfs_set_wait_limit), read once per
+// CTA at kernel start.
 constexpr uint64_t kWaitLimitNs = 1000000000ull;
+// Limit of the waits that drain a CTA's own copies and products after a wait
+// gave up; independent of the handle's limit so that the drain completes.
+constexpr uint64_t kDrainLimitNs = 1000000000ull;
 
 // Bounded wait for the phase with the given parity (try_wait may suspend the
-// thread between polls); false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// thread between polls); false once lim ns have passed since the first
+// failed poll.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t lim) {
   uint64_t t0 = 0;
   for (;;) {
     uint32_t done;
@@ -78,13 +84,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (done) return true;
     const uint64_t t = global_ns();  // the clock is read only once a poll has failed
     if (t0 == 0) t0 = t;
-    else if (t - t0 > kWaitLimitNs) return false;
+    else if (t - t0 > lim) return false;
   }
 }
 
 // Bounded spin without suspension, for the single producer / MMA threads whose
-// waits sit on the critical path of every K block; false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity) {
+// waits sit on the critical path of every K block; false once lim ns have
+// passed (the clock is read every 256 polls).
+__device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity, uint64_t lim) {
   uint64_t t0 = 0;
   for (uint32_t it = 0;; ++it) {
     uint32_t done;
@@ -99,7 +106,7 @@ __device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity) {
     if ((it & 255) == 255) {  // no clock read on the fast path
       const uint64_t t = global_ns();
       if (t0 == 0) t0 = t;
-      else if (t - t0 > kWaitLimitNs) return false;
+      else if (t - t0 > lim) return false;
     }
   }
 }
@@ -107,7 +114,7 @@ __device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity) {
 // A wait that gave up: flag the error (bit 2 of status[0]) and, for the first
 // one, record where: status[1] = role (1 producer/stage free, 2 MMA/accumulator
 // free, 3 MMA/stage loaded, 4 epilogue/accumulator ready), status[2] = block,
-// status[3] = pipeline step.
+// status[3] = pipeline step. A drain wait that gave up sets bit 4.
 __device__ __forceinline__ void report_timeout(int* status, int role, int step) {
   atomicOr(status, 2);
   if (atomicCAS(status + 1, 0, role) == 0) {
@@ -366,7 +373,8 @@ __device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t tr
 
 __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* __restrict__ descs,
                                                             const TcWork* __restrict__ work, int nwork,
-                                                            int* __restrict__ status) {
+                                                            int* __restrict__ status,
+                                                            const unsigned long long* __restrict__ wait_ns) {
   constexpr int BK = 64, S = 2, AB = 128 * BK * 2, SB = kPStage;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -377,6 +385,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
   const uint32_t sbase = smem_u32(smem);
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]);
   const uint32_t accf0 = smem_u32(&bars[4]), acce0 = smem_u32(&bars[6]);
+  const uint64_t lim = *wait_ns;
   if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 256);
   if (tid == 0) {
     for (int b = 0; b < 6; b++) mbar_init(smem_u32(&bars[b]), 1);
@@ -399,7 +408,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       const int ns = d.nprod == 3 ? 2 : 3;  // slices per operand
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g & 1;
-        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g >> 1) + 1) & 1)) { report_timeout(status, 1, g); to = true; break; }
+        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g >> 1) + 1) & 1, lim)) { report_timeout(status, 1, g); to = true; break; }
         const uint32_t fb = full0 + 8 * s;
         mbar_expect_tx(fb, 2 * ns * AB);
         const uint32_t st = sbase + s * SB;
@@ -407,6 +416,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
         for (int t = 0; t < ns; t++) tma_load_3d(st + 3 * AB + t * AB, &d.mapB, kb * BK, n0, t, fb);
       }
     }
+    // Drain: only the last S stage loads can still be in flight (a stage is
+    // reloaded only after the MMAs that read it completed, which waited for
+    // its load). Their full-barrier phases complete when their bytes land;
+    // in a run without timeouts they have completed already.
+    for (int gi = g - 1; gi >= 0 && gi >= g - S; gi--)
+      if (!mbar_spin(full0 + 8 * (gi & 1), (gi >> 1) & 1, kDrainLimitNs)) atomicOr(status, 4);
   } else if (tid == 32) {  // MMA issuer
     constexpr int pa[6] = {0, 0, 1, 0, 1, 2};
     constexpr int pb[6] = {0, 1, 0, 2, 1, 0};
@@ -414,9 +429,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     // the descriptor never carries into the next field
     const uint64_t d0 = smem_desc_kmajor<BK>(sbase);
     int g = 0, t = 0;
+    uint32_t last_bar = 0, last_par = 0;  // barrier and phase parity of the last commit
     for (int w = blockIdx.x; w < nwork && !to; w += G, t++) {
       const int a = t & 1, u = t >> 1;
-      if (t >= 2 && !mbar_spin(acce0 + 8 * a, (u - 1) & 1)) { report_timeout(status, 2, t); to = true; break; }
+      if (t >= 2 && !mbar_spin(acce0 + 8 * a, (u - 1) & 1, lim)) { report_timeout(status, 2, t); to = true; break; }
       tc_fence_after();
       const TcDesc& d = descs[work[w].desc];
       const int nk = d.Kp / BK;
@@ -424,7 +440,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       const uint32_t acc = tmem + a * 128;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g & 1;
-        if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1)) { report_timeout(status, 3, g); to = true; break; }
+        if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1, lim)) { report_timeout(status, 3, g); to = true; break; }
         tc_fence_after();
         // stage base descriptor; operand tiles and K steps are immediate
         // offsets (16-byte units) on its address field
@@ -439,9 +455,18 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
                            (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
         }
         umma_commit(empty0 + 8 * s);
+        last_bar = empty0 + 8 * s;
+        last_par = (g >> 1) & 1;
       }
-      if (!to) umma_commit(accf0 + 8 * a);
+      if (!to) {
+        umma_commit(accf0 + 8 * a);
+        last_bar = accf0 + 8 * a;
+        last_par = u & 1;
+      }
     }
+    // Drain: a commit's barrier phase completes once every MMA this thread
+    // issued before it has completed; TMEM is freed only after that.
+    if (last_bar && !mbar_spin(last_bar, last_par, kDrainLimitNs)) atomicOr(status, 4);
   } else if (warp >= 2) {  // epilogue warps
     const int q = warp & 3;              // TMEM lane quarter this warp may access
     const int c0 = ((warp - 2) >> 2) * 2;  // the warp's two 32-column chunks
@@ -449,7 +474,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     int t = 0;
     for (int w = blockIdx.x; w < nwork; w += G, t++) {
       const int a = t & 1, u = t >> 1;
-      if (!mbar_wait(accf0 + 8 * a, u & 1)) { report_timeout(status, 4, t); to = true; break; }
+      if (!mbar_wait(accf0 + 8 * a, u & 1, lim)) { report_timeout(status, 4, t); to = true; break; }
       tc_fence_after();
       const TcDesc& d = descs[work[w].desc];
       const int tile = work[w].tile;
@@ -588,6 +613,7 @@ struct PrecisionPlan {
   std::map<int, std::pair<bf16*, long long>> sine;  // N+1 -> slices
   std::map<int, float*> lam;                        // N+1 -> 1-D eigenvalues
   int* status = nullptr;
+  unsigned long long* wait_ns = nullptr;  // limit of the GEMM's waits, ns (device word)
   Alloc alloc;
 };
 
@@ -676,6 +702,15 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
   }
   pp->status = cases.empty() ? (int*)alloc(sizeof(int) * 4) : cases[0].status;
+  pp->wait_ns = (unsigned long long*)alloc(sizeof(unsigned long long));
+  if (!pp->wait_ns) {
+    g_perr = "device allocation failed for the wait limit";
+    return 8;
+  }
+  if (precision_set_wait_limit(pp, (double)kWaitLimitNs * 1e-9)) {
+    g_perr = "cannot set the wait limit";
+    return 4;
+  }
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
     void* fn = nullptr;
@@ -720,6 +755,12 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
 }
 
 void precision_free(PrecisionPlan* pp) { delete pp; }
+
+int precision_set_wait_limit(PrecisionPlan* pp, double seconds) {
+  if (!pp || !pp->wait_ns || !(seconds >= 0.0) || seconds > 60.0) return 7;
+  const unsigned long long ns = (unsigned long long)(seconds * 1e9);
+  return cudaMemcpy(pp->wait_ns, &ns, sizeof(ns), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : 4;
+}
 const char* precision_error() { return g_perr.c_str(); }
 
 // One solve request: x = A^-1 v for one (case, level) item.
@@ -757,7 +798,8 @@ static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDes
   int nw = (int)wl.size();
   int grid = std::min(nw, g_num_sms > 0 ? g_num_sms : 148);
   int* status = pp->status;
-  P.push_back({[=]() { k_gemm_tc_persist<<<grid, kPThreads, kPSmem, st>>>(dd, dw, nw, status); }, TAG_GEMM_TC, fl});
+  const unsigned long long* wait_ns = pp->wait_ns;
+  P.push_back({[=]() { k_gemm_tc_persist<<<grid, kPThreads, kPSmem, st>>>(dd, dw, nw, status, wait_ns); }, TAG_GEMM_TC, fl});
 }
 
 static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all, cudaStream_t st) {

@@ -230,24 +230,32 @@ int main(int argc, char** argv) {
       std::vector<double*> parts;
       for (size_t c : cnt) buf.emplace_back(c);
       for (auto& b : buf) parts.push_back(b.data());
-      if (!read_record(var_name(p.istart), parts, cnt, msg)) return stop(msg, 2);
+      if (!read_record(var_name(p.istart), parts, cnt, msg)) return stop(msg, IBFS_ERR_IO);
       for (auto& b : buf) {
         double s = 0.0;
         for (double v : b) s += v;
         var_sums.push_back(s);
       }
     }
+    // the Cholesky record a stationary run would read (variables.f90:110-137)
+    int chd_ok = -1;  // -1: no file
+    if (p.stationary && file_exists("input/ibfs.chd")) {
+      std::vector<double> cm((size_t)4 * nb * nb), cv((size_t)2 * nb);
+      if (!read_record("input/ibfs.chd", {cm.data(), cv.data()}, {cm.size(), cv.size()}, msg))
+        return stop("input/ibfs.chd: " + msg, IBFS_ERR_IO);
+      chd_ok = 1;
+    }
     std::printf("{\"istart\": %d, \"istop\": %d, \"isave\": %d, \"m\": %d, \"n\": %d, \"dt\": %.17g, "
                 "\"re\": %.17g, \"cgtol\": %.17g, \"cg_max_iter\": %d, \"unif_flow\": %d, \"len\": %.17g, "
                 "\"offsetx\": %.17g, \"offsety\": %.17g, \"mgridlev\": %d, \"make_vortex\": %d, "
                 "\"stationary\": %d, \"precision\": %d, \"cg_relative\": %d, \"motion_kind\": %d, "
                 "\"tile_cfg\": %d, \"cg_precond\": %d, \"nb\": %d, \"x0\": %.17g, \"y0\": %.17g, \"xsum\": %.17g, \"ysum\": %.17g, "
-                "\"n_act\": %d, \"n_act_pt\": %d, \"var_sums\": [",
+                "\"n_act\": %d, \"n_act_pt\": %d, \"chd_ok\": %d, \"var_sums\": [",
                 p.istart, p.istop, p.isave, p.m, p.n, p.dt, p.re, p.cgtol, p.cg_max_iter, p.unif_flow, p.len,
                 p.offsetx, p.offsety, p.mgridlev, p.make_vortex, p.stationary, opt.precision, opt.cg_relative,
                 opt.motion_kind, opt.tile_cfg, opt.cg_precond, nb, nb ? geo.x[0] : 0.0, nb ? geo.y[0] : 0.0,
                 [&] { double t = 0.0; for (double v : geo.x) t += v; return t; }(),
-                [&] { double t = 0.0; for (double v : geo.y) t += v; return t; }(), n_act, n_act_pt);
+                [&] { double t = 0.0; for (double v : geo.y) t += v; return t; }(), n_act, n_act_pt, chd_ok);
     for (size_t i = 0; i < var_sums.size(); i++) std::printf("%s%.17g", i ? ", " : "", var_sums[i]);
     std::printf("]}\n");
     return 0;
@@ -283,7 +291,7 @@ int main(int argc, char** argv) {
       if (it > 0) {
         if (!read_record(var_name(it), {omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data()},
                          {omega.size(), fb.size(), rhs_old.size(), q.size(), q0.size()}, msg))
-          return stop(msg, 5);
+          return stop(msg, IBFS_ERR_IO);
         rc = ibfs_set_state(h, 0, omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data());
         if (rc) return stop(std::string("ibfs_set_state: ") + ibfs_last_error(h), 10 + rc);
       }
@@ -295,7 +303,7 @@ int main(int argc, char** argv) {
         std::snprintf(name, sizeof name, "post/ibfs_g%1dt%07d_vel.dat", k, it);
         if (!write_tecplot(name, it, m, n, (double)(float)(1 << (k - 1)), p.len / (double)p.m, p.len,
                            p.offsetx, p.offsety, fields.data(), msg))
-          return stop(msg, 5);
+          return stop(msg, IBFS_ERR_IO);
       }
     }
     ibfs_destroy(h);
@@ -305,12 +313,12 @@ int main(int argc, char** argv) {
   if (p.istart > 0) {
     if (!read_record(var_name(p.istart), {omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data()},
                      {omega.size(), fb.size(), rhs_old.size(), q.size(), q0.size()}, msg))
-      return stop(msg, 5);
+      return stop(msg, IBFS_ERR_IO);
     rc = ibfs_set_state(h, 0, omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data());
     if (rc) return stop(std::string("ibfs_set_state: ") + ibfs_last_error(h), 10 + rc);
     logline("Reading restart file at itime= " + std::to_string(p.istart));
     std::printf("Reading restart file at itime = %d\n", p.istart);
-    if (p.stationary && !read_chd()) return stop("input/ibfs.chd: " + msg, 5);
+    if (p.stationary && !read_chd()) return stop("input/ibfs.chd: " + msg, IBFS_ERR_IO);
   }
 
   // TIME MARCH (main.f90:45-50)
@@ -320,7 +328,7 @@ int main(int argc, char** argv) {
   while (it < p.istop) {
     if (it + 1 == 1 && p.stationary) {  // preprocess (operators.f90:88-90)
       if (file_exists("input/ibfs.chd")) {
-        if (!read_chd()) return stop("input/ibfs.chd: " + msg, 5);
+        if (!read_chd()) return stop("input/ibfs.chd: " + msg, IBFS_ERR_IO);
       } else {
         std::printf("Precomputing body matrix...\n");
         logline("Precomputing body matrix...");
@@ -329,7 +337,7 @@ int main(int argc, char** argv) {
         ibfs_get_cholesky(h, 0, cholmat.data(), cholvec.data());
         if (!write_record("input/ibfs.chd", {cholmat.data(), cholvec.data()}, {cholmat.size(), cholvec.size()},
                           msg))
-          return stop(msg, 5);
+          return stop(msg, IBFS_ERR_IO);
         logline("Saving cholesky decomposition...");
       }
     }
@@ -346,7 +354,7 @@ int main(int argc, char** argv) {
       ibfs_get_state(h, 0, omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data());
       if (!write_record(var_name(it), {omega.data(), fb.data(), rhs_old.data(), q.data(), q0.data()},
                         {omega.size(), fb.size(), rhs_old.size(), q.size(), q0.size()}, msg))
-        return stop(msg, 5);
+        return stop(msg, IBFS_ERR_IO);
       logline("Writing restart file at itime= " + std::to_string(it));
     }
     std::vector<double> fv;

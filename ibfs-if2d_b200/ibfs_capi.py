@@ -26,7 +26,7 @@ EXPORTS = [
     "ibfs_advance", "ibfs_advance_n", "ibfs_batch_advance", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
     "ibfs_last_cg_iterations", "ibfs_adjoint_run", "ibfs_adjoint_pitch_run", "ibfs_vertex_fields",
-    "ibfs_set_actuators",
+    "ibfs_set_actuators", "ibfs_set_wait_limit",
     "ibfs_last_error",
 ]
 
@@ -97,6 +97,7 @@ def lib():
         L.ibfs_adjoint_pitch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]
         L.ibfs_set_actuators.argtypes = [vp, ctypes.c_int, ctypes.c_int, _IP, _DP, _DP, _DP, _DP]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
+        L.ibfs_set_wait_limit.argtypes = [vp, ctypes.c_double]
         L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
         L.ibfs_last_error.argtypes = [vp]
@@ -301,6 +302,10 @@ class Solver:
         if nc == 1:
             return float(J[0]), float(dJ[0]), ms_f.value, ms_t.value
         return J, dJ, ms_f.value, ms_t.value
+
+    def set_wait_limit(self, seconds):
+        """Limit of the bounded device waits (ibfs_set_wait_limit)."""
+        self._check(lib().ibfs_set_wait_limit(self.h, float(seconds)))
 
     def last_cg_iterations(self):
         return lib().ibfs_last_cg_iterations(self.h)

@@ -72,6 +72,30 @@ def batch(ncases=256, seed=20261203):
     return out
 
 
+def strata(cases):
+    """The batch grouped by (grid size m, level count L): {(m, L): [case
+    indices]}, in batch order within each group."""
+    out = {}
+    for i, c in enumerate(cases):
+        out.setdefault((c["m"], c["levels"]), []).append(i)
+    return dict(sorted(out.items()))
+
+
+def stratified_sample(cases, body=None):
+    """One case per (m, L) stratum of the batch: the first case of the body
+    type `body` ("plate", "cylinder") in each stratum, or, with body None,
+    alternately the first plate and the first cylinder (strata in (m, L)
+    order), falling back to the stratum's first case. Returns (indices,
+    weights), the weight being the stratum's share of the batch's cases."""
+    ids, wts = [], []
+    for s, (key, members) in enumerate(strata(cases).items()):
+        want = body if body is not None else ("plate" if s % 2 == 0 else "cylinder")
+        pick = next((i for i in members if cases[i]["body"] == want), members[0])
+        ids.append(pick)
+        wts.append(len(members))
+    return ids, wts
+
+
 def cells_per_step(cases, nlev):
     """Cell-updates per step: sum of L*m*n over cases (levels after the clamp)."""
     return int(sum(L * c["m"] * c["n"] for c, L in zip(cases, nlev)))

@@ -86,7 +86,60 @@ def test_restart_record(tmp_path):
     # a record too short for the grid is refused
     fortran_record(tmp_path / "output" / "ibfs0000012.var", parts[:3])
     rc, out, err = run(tmp_path)
-    assert rc != 0 and "record holds" in err
+    assert rc == IBFS_ERR_IO and "record holds" in err
+
+
+IBFS_ERR_IO = 5  # include/ibfs_capi.h; the driver's exit status for a file it cannot use
+
+
+def test_truncated_and_corrupt_records_are_io_errors(tmp_path):
+    """Restart (.var, variables.f90:141-175) and Cholesky (.chd, :110-137)
+    records cut short or with broken record markers stop the driver with
+    IBFS_ERR_IO, as the reference's READ would stop on a bad record."""
+    m = n = 32
+    L = 3
+    write_inp(tmp_path, f"&READ_PARAMETERS ISTART=12, ISTOP=14, M={m}, N={n}, MGRIDLEV={L}, LEN=4., "
+                        "OFFSETX=2., OFFSETY=2., STATIONARY=T /\n")
+    (tmp_path / "input" / "geom.inp").write_text("2\n 0.0 0.0 0\n 0.1 0.0 0\n")
+    os.makedirs(tmp_path / "output", exist_ok=True)
+    ns, nq, nf = (m - 1) * (n - 1), (m + 1) * n + (n + 1) * m, 4
+    rng = np.random.default_rng(4)
+    parts = [rng.standard_normal(ns * L), rng.standard_normal(nf), rng.standard_normal(ns * L),
+             rng.standard_normal(nq * L), rng.standard_normal(nq * L)]
+    var = tmp_path / "output" / "ibfs0000012.var"
+    chd = tmp_path / "input" / "ibfs.chd"
+    fortran_record(var, parts)
+    fortran_record(chd, [rng.standard_normal(nf * nf), rng.standard_normal(nf)])
+    rc, out, err = run(tmp_path)
+    assert rc == 0, err
+    assert json.loads(out)["chd_ok"] == 1
+    good_var, good_chd = var.read_bytes(), chd.read_bytes()
+    # .var cut in the middle of its payload: the trailing record marker is missing
+    var.write_bytes(good_var[:len(good_var) // 2])
+    rc, out, err = run(tmp_path)
+    assert rc == IBFS_ERR_IO and "corrupt record markers" in err, (rc, err)
+    # .var with only its leading marker
+    var.write_bytes(good_var[:4])
+    rc, out, err = run(tmp_path)
+    assert rc == IBFS_ERR_IO, (rc, err)
+    # empty .var
+    var.write_bytes(b"")
+    rc, out, err = run(tmp_path)
+    assert rc == IBFS_ERR_IO and "truncated record" in err, (rc, err)
+    var.write_bytes(good_var)
+    # .chd truncated, then with a trailing marker that disagrees with the leading one
+    chd.write_bytes(good_chd[:-12])
+    rc, out, err = run(tmp_path)
+    assert rc == IBFS_ERR_IO and "ibfs.chd" in err, (rc, err)
+    bad = bytearray(good_chd)
+    bad[-4:] = struct.pack("<i", 8)
+    chd.write_bytes(bytes(bad))
+    rc, out, err = run(tmp_path)
+    assert rc == IBFS_ERR_IO and "corrupt record markers" in err, (rc, err)
+    # a .chd record for a smaller body (fewer forces than the geometry has)
+    fortran_record(chd, [rng.standard_normal(4), rng.standard_normal(2)])
+    rc, out, err = run(tmp_path)
+    assert rc == IBFS_ERR_IO and "record holds" in err, (rc, err)
 
 
 def test_bad_namelist(tmp_path):
