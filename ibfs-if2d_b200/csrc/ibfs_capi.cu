@@ -397,6 +397,7 @@ static void build_atimes_d(ProgBuilder& B, ibfs_handle* h, double** d_out) {
 
 static void build_step_program(ibfs_handle* h) {
   h->prog.clear();
+  if (h->prec) precision_reset_tile_choices(h->prec);
   ProgBuilder B{h, h->prog};
   cudaStream_t st = h->st;
   const DevCase* dcases = h->d_cases;
@@ -960,7 +961,25 @@ static int setup_case(ibfs_handle* h, HostCase& c, const ibfs_params_c& p, const
       for (size_t t = 0; t < (size_t)(c.m + 1) * c.n; t++) q0[t + (k - 1) * c.nq] = c.delta * std::pow(2.0, k - 1);
     cudaMemcpy(d.q0, q0.data(), sizeof(double) * nqL, cudaMemcpyHostToDevice);
   }
+  d.q0_const = 1;
+  d.q0_u1 = p.unif_flow ? c.delta : 0.0;
   return IBFS_OK;
+}
+
+// Whether a q0 array (L levels of Nq faces) is q0_u1 * 2^(k-1) on the u-faces
+// of every level k and 0 on the v-faces, for q0_u1 = its first value.
+static bool q0_closed_form(const HostCase& c, const double* q0, double* u1) {
+  const size_t nu = (size_t)(c.m + 1) * c.n;
+  *u1 = q0[0];
+  for (int k = 1; k <= c.L; k++) {
+    const double* lv = q0 + (size_t)(k - 1) * c.nq;
+    const double uk = *u1 * std::pow(2.0, k - 1);
+    for (size_t t = 0; t < nu; t++)
+      if (lv[t] != uk) return false;
+    for (size_t t = nu; t < (size_t)c.nq; t++)
+      if (lv[t] != 0.0) return false;
+  }
+  return true;
 }
 
 static int finish_create(ibfs_handle* h) {
@@ -1058,6 +1077,7 @@ static int finish_create(ibfs_handle* h) {
       return p;
     });
     if (rc) return fail(rc, precision_error());
+    precision_set_tile(h->prec, h->cases[0].o.tc_tile);
   }
   build_step_program(h);
   IBFS_CUDA_CHECK(cudaDeviceSynchronize());
@@ -1183,7 +1203,19 @@ int ibfs_case_sizes(const ibfs_handle* h, int icase, int* m, int* n, int* nlev, 
 int ibfs_set_state(ibfs_handle* h, int icase, const double* omega, const double* fb, const double* rhs_old,
                    const double* q, const double* q0) {
   if (!h || icase < 0 || icase >= (int)h->cases.size()) return IBFS_ERR_ARG;
-  const HostCase& c = h->cases[icase];
+  HostCase& c = h->cases[icase];
+  if (q0) {  // the stencils read q0 from the array unless it has the closed form
+    double u1 = 0.0;
+    const int cf = q0_closed_form(c, q0, &u1) ? 1 : 0;
+    if (cf != c.dc.q0_const || (cf && u1 != c.dc.q0_u1)) {
+      c.dc.q0_const = cf;
+      c.dc.q0_u1 = cf ? u1 : 0.0;
+      IBFS_CUDA_CHECK(cudaMemcpyAsync(&h->d_cases[icase].q0_const, &c.dc.q0_const, sizeof(int),
+                                      cudaMemcpyHostToDevice, h->st));
+      IBFS_CUDA_CHECK(cudaMemcpyAsync(&h->d_cases[icase].q0_u1, &c.dc.q0_u1, sizeof(double),
+                                      cudaMemcpyHostToDevice, h->st));
+    }
+  }
   size_t nsL = (size_t)c.L * c.ns, nqL = (size_t)c.L * c.nq;
   auto cp = [&](double* d, const double* s, size_t n) {
     return s ? cudaMemcpyAsync(d, s, n * sizeof(double), cudaMemcpyHostToDevice, h->st) : cudaSuccess;
@@ -1370,6 +1402,14 @@ int ibfs_output_offset(const ibfs_handle* h, int icase) {
 int ibfs_output_stride(const ibfs_handle* h) { return h ? h->out_stride : 0; }
 
 int ibfs_kernels_per_step(const ibfs_handle* h) { return h ? h->graph_kernels : -1; }
+
+int ibfs_gemm_tiles(const ibfs_handle* h, int* widths, int max) {
+  if (!h) return -1;
+  if (!h->prec) return 0;
+  const std::vector<int>& w = precision_tile_choices(h->prec);
+  for (int i = 0; widths && i < (int)w.size() && i < max; i++) widths[i] = w[i];
+  return (int)w.size();
+}
 
 int ibfs_last_cg_iterations(const ibfs_handle* h) { return h ? h->last_cg_iters : -1; }
 

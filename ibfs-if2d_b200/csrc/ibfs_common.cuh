@@ -22,6 +22,11 @@ struct DevCase {
   double delta, dt, re, norm;
   // state
   double *omega, *rhs_old, *q, *q0, *fb;
+  // q0 known in closed form: 1 when every level k holds q0_u1 * 2^(k-1) on
+  // its u-faces and 0 on its v-faces (uniform flow, variables.f90:60-64, with
+  // q0_u1 = delta; or no flow, q0_u1 = 0), so the stencils need not read it
+  int q0_const;
+  double q0_u1;
   // per-level work
   double *s;       // [L][ns] streamfunction per level
   double *lastbc;  // [L][nring]

@@ -63,6 +63,19 @@ __host__ __device__ inline int coarsify_count(int m, int n) {
 void launch_vertex(const DevCase* cases, int c, int k, int ns, double* out, cudaStream_t st);
 void launch_rhs(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, int first,
                 cudaStream_t st);
+// Split-precision level update input (k_rhs_split): per (case, level) item,
+// b = scale * rhsA + (omega_k - nu C^T C omega_k) into b64 (FP64, column-major)
+// and three BF16 slices Xs [slice][i][j] (row stride ld, slice stride sX).
+struct RhsSplitDesc {
+  double scale, nu;
+  double* b64;
+  uint16_t* Xs;
+  long long sX;
+  int ld;
+};
+// one block per 32 x 32 node tile: bmap[b] = {item, tile}, tiles i-fastest
+void launch_rhs_split(const DevCase* cases, const LevelItem* items, const RhsSplitDesc* sd, const int2* bmap,
+                      int nblocks, int first, cudaStream_t st);
 void launch_coarsify(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, cudaStream_t st);
 void launch_curl(const DevCase* cases, const LevelItem* items, const int2* bmap, int nblocks, cudaStream_t st);
 void launch_regrot(const DevCase* cases, const int* cids, const int2* bmap, int nblocks, cudaStream_t st);

@@ -19,6 +19,11 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t st, const std::vector<DevCas
 void precision_free(PrecisionPlan* pp);
 // Limit (seconds, 0..60) of every bounded wait of the tensor-core GEMM.
 int precision_set_wait_limit(PrecisionPlan* pp, double seconds);
+// Output tile width of the tensor-core GEMM: 128, 256, or 0 for the autotuner.
+void precision_set_tile(PrecisionPlan* pp, int width);
+// Widths chosen for the GEMM launch groups built since the last reset.
+const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp);
+void precision_reset_tile_choices(PrecisionPlan* pp);
 const char* precision_error();
 void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, const std::vector<DevCase>& cs,
                            cudaStream_t st);

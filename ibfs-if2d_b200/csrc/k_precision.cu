@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -199,13 +200,17 @@ enum TcEpi { TC_SPLIT_COL = 0, TC_SCALE_SPLIT_ROW = 1, TC_F64_STORE = 2, TC_F64_
 enum TcFactor { F_NONE = 0, F_LAMINV = 1, F_LAM1I_NORM = 2 };
 
 // One GEMM of one (case, level) item. Operands are 3-slice BF16 arrays
-// [slice][row][k] (k contiguous) described by TMA tensor maps (box 32 k x 128
-// rows, 64-byte swizzle); A rows are output rows, B rows output columns.
+// [slice][row][k] (k contiguous) described by TMA tensor maps; A rows are
+// output rows, B rows output columns. mapA/mapB serve the 128 x 128 output
+// tile (box 64 k x 128 rows, 128-byte swizzle), mapA2/mapB2 the 128 x 256
+// tile (box 32 k x 128 / 256 rows, 64-byte swizzle).
 struct __align__(64) TcDesc {
   CUtensorMap mapA;
   CUtensorMap mapB;
+  CUtensorMap mapA2;
+  CUtensorMap mapB2;
   int M, N, Kp;   // logical output extents; K padded to a multiple of 64
-  int tiles_m, tiles_n, bn;
+  int tiles_m;    // 128-row output tiles
   int nprod;      // slice products: 6 (three slices per operand) or 3 (two slices: A0B0 + A0B1 + A1B0)
   int epi, fkind;
   int ldcs, ldc;
@@ -263,12 +268,20 @@ struct TcWork {
   int desc, tile;
 };
 
-constexpr int kPStage = 3 * 128 * 64 * 2 + 3 * 128 * 64 * 2;  // 96 KB
+// Output tile 128 x BN: BN = 128 with K blocks of 64 (128-byte rows), or
+// BN = 256 with K blocks of 32 (64-byte rows); two pipeline stages each.
+template <int BN> struct TcShape;
+template <> struct TcShape<128> { static constexpr int BK = 64; };
+template <> struct TcShape<256> { static constexpr int BK = 32; };
+template <int BN> constexpr int tc_ab() { return 128 * TcShape<BN>::BK * 2; }   // one A slice tile
+template <int BN> constexpr int tc_bb() { return BN * TcShape<BN>::BK * 2; }    // one B slice tile
+template <int BN> constexpr int tc_stage() { return 3 * tc_ab<BN>() + 3 * tc_bb<BN>(); }  // 96 KB / 72 KB
 constexpr int kPEpiWarps = 8;                                  // two warps per TMEM lane quarter
 constexpr int kPThreads = 64 + 32 * kPEpiWarps;
 constexpr int kPEpi = kPEpiWarps * 32 * 33 * 4;                // per-warp 32 x 33 FP32 staging
-constexpr int kPSmem = 2 * kPStage + kPEpi + 1024 + 256;
-static_assert(kPSmem <= 232448, "persistent GEMM shared memory above the per-CTA limit");
+template <int BN> constexpr int tc_smem() { return 2 * tc_stage<BN>() + kPEpi + 1024 + 256; }
+static_assert(tc_smem<128>() <= 232448, "persistent GEMM shared memory above the per-CTA limit");
+static_assert(tc_smem<256>() <= 232448, "persistent GEMM shared memory above the per-CTA limit");
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
@@ -371,11 +384,13 @@ __device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t tr
   }
 }
 
+template <int BN>
 __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* __restrict__ descs,
                                                             const TcWork* __restrict__ work, int nwork,
                                                             int* __restrict__ status,
                                                             const unsigned long long* __restrict__ wait_ns) {
-  constexpr int BK = 64, S = 2, AB = 128 * BK * 2, SB = kPStage;
+  constexpr int BK = TcShape<BN>::BK, S = 2, AB = tc_ab<BN>(), BB = tc_bb<BN>(), SB = tc_stage<BN>();
+  constexpr uint32_t TCOLS = 2 * BN;  // double-buffered FP32 accumulator columns
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   float* stg_all = reinterpret_cast<float*>(smem + S * SB);
@@ -386,7 +401,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]);
   const uint32_t accf0 = smem_u32(&bars[4]), acce0 = smem_u32(&bars[6]);
   const uint64_t lim = *wait_ns;
-  if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 256);
+  if (warp == 0) tmem_alloc(smem_u32(tmem_slot), TCOLS);
   if (tid == 0) {
     for (int b = 0; b < 6; b++) mbar_init(smem_u32(&bars[b]), 1);
     for (int b = 6; b < 8; b++) mbar_init(smem_u32(&bars[b]), kPEpiWarps);
@@ -403,17 +418,19 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     for (int w = blockIdx.x; w < nwork && !to; w += G) {
       const TcDesc& d = descs[work[w].desc];
       const int tile = work[w].tile;
-      const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * 128;
+      const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * BN;
       const int nk = d.Kp / BK;
       const int ns = d.nprod == 3 ? 2 : 3;  // slices per operand
+      const CUtensorMap* mA = BN == 128 ? &d.mapA : &d.mapA2;
+      const CUtensorMap* mB = BN == 128 ? &d.mapB : &d.mapB2;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g & 1;
         if (g >= S && !mbar_spin(empty0 + 8 * s, ((g >> 1) + 1) & 1, lim)) { report_timeout(status, 1, g); to = true; break; }
         const uint32_t fb = full0 + 8 * s;
-        mbar_expect_tx(fb, 2 * ns * AB);
+        mbar_expect_tx(fb, ns * (AB + BB));
         const uint32_t st = sbase + s * SB;
-        for (int t = 0; t < ns; t++) tma_load_3d(st + t * AB, &d.mapA, kb * BK, m0, t, fb);
-        for (int t = 0; t < ns; t++) tma_load_3d(st + 3 * AB + t * AB, &d.mapB, kb * BK, n0, t, fb);
+        for (int t = 0; t < ns; t++) tma_load_3d(st + t * AB, mA, kb * BK, m0, t, fb);
+        for (int t = 0; t < ns; t++) tma_load_3d(st + 3 * AB + t * BB, mB, kb * BK, n0, t, fb);
       }
     }
     // Drain: only the last S stage loads can still be in flight (a stage is
@@ -437,7 +454,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       const TcDesc& d = descs[work[w].desc];
       const int nk = d.Kp / BK;
       const int np = d.nprod == 3 ? 3 : 6;
-      const uint32_t acc = tmem + a * 128;
+      const uint32_t acc = tmem + a * BN;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g & 1;
         if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1, lim)) { report_timeout(status, 3, g); to = true; break; }
@@ -450,9 +467,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
           if (p >= np) break;
 #pragma unroll
           for (int k16 = 0; k16 < BK / 16; k16++)
-            umma_bf16<128>(acc, ds + (uint64_t)((pa[p] * AB + k16 * 32) >> 4),
-                           ds + (uint64_t)((3 * AB + pb[p] * AB + k16 * 32) >> 4),
-                           (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
+            umma_bf16<BN>(acc, ds + (uint64_t)((pa[p] * AB + k16 * 32) >> 4),
+                          ds + (uint64_t)((3 * AB + pb[p] * BB + k16 * 32) >> 4),
+                          (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
         }
         umma_commit(empty0 + 8 * s);
         last_bar = empty0 + 8 * s;
@@ -468,8 +485,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     // issued before it has completed; TMEM is freed only after that.
     if (last_bar && !mbar_spin(last_bar, last_par, kDrainLimitNs)) atomicOr(status, 4);
   } else if (warp >= 2) {  // epilogue warps
-    const int q = warp & 3;              // TMEM lane quarter this warp may access
-    const int c0 = ((warp - 2) >> 2) * 2;  // the warp's two 32-column chunks
+    const int q = warp & 3;                       // TMEM lane quarter this warp may access
+    constexpr int CH = BN / 64;                   // 32-column chunks per warp
+    const int c0 = ((warp - 2) >> 2) * CH;        // the warp's half of the tile's columns
     float* stg = stg_all + (warp - 2) * (32 * 33);
     int t = 0;
     for (int w = blockIdx.x; w < nwork; w += G, t++) {
@@ -478,9 +496,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       tc_fence_after();
       const TcDesc& d = descs[work[w].desc];
       const int tile = work[w].tile;
-      const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * 128;
+      const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * BN;
       const int r0 = m0 + 32 * q;
-      tc_epilogue(d, n0, tmem + a * 128 + ((uint32_t)(32 * q) << 16), r0, lane, stg, c0, c0 + 2);
+      tc_epilogue(d, n0, tmem + a * BN + ((uint32_t)(32 * q) << 16), r0, lane, stg, c0, c0 + CH);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce0 + 8 * a);
@@ -490,7 +508,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
   __syncthreads_or(to);
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, TCOLS);
 }
 
 // ---------------------------------------------------------------------------
@@ -602,10 +620,10 @@ struct CaseBufs {
   const bf16* Sn;
   long long sSm, sSn;
   int ldSm, ldSn;
-  CUtensorMap mapX, mapT, mapSm, mapSn;
+  CUtensorMap mapX, mapT, mapSm, mapSn;      // K blocks of 64: A roles 128 rows, B roles 128 rows
+  CUtensorMap mapX2, mapT2, mapSm2, mapSn2;  // K blocks of 32: A roles 128 rows, B roles 256 rows
   const float* lamx;
   const float* lamy;
-  int bn;  // output tile width of this case's GEMMs (128)
 };
 
 struct PrecisionPlan {
@@ -614,6 +632,8 @@ struct PrecisionPlan {
   std::map<int, float*> lam;                        // N+1 -> 1-D eigenvalues
   int* status = nullptr;
   unsigned long long* wait_ns = nullptr;  // limit of the GEMM's waits, ns (device word)
+  int tc_tile = 0;                        // output tile width: 0 = the measured autotuner, 128 or 256
+  std::vector<int> tile_choice;           // width used by each GEMM launch group, in build order
   Alloc alloc;
 };
 
@@ -692,7 +712,10 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   pp->alloc = alloc;
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_gemm_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, kPSmem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_gemm_tc_persist<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc_persist<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<256>()) !=
+            cudaSuccess) {
       g_perr = "cannot raise shared memory limit for the tensor-core GEMM";
       return 4;
     }
@@ -722,9 +745,8 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   }
   for (auto& c : cases) {
     CaseBufs b{};
-    b.bn = 128;
-    const int bk = 64;
-    int Rm = rup(c.m - 1, 128), Rn = rup(c.n - 1, b.bn), Km = rup(c.m - 1, 64), Kn = rup(c.n - 1, 64);
+    // T is the B operand of the left GEMMs: rows padded to the widest tile
+    int Rm = rup(c.m - 1, 128), Rn = rup(c.n - 1, 256), Km = rup(c.m - 1, 64), Kn = rup(c.n - 1, 64);
     b.sX = (long long)Rm * Kn;
     b.sT = (long long)Rn * Km;
     b.ldX = Kn;
@@ -742,10 +764,11 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
       return 8;
     }
     const int Rs_m = rup(c.m - 1, 256), Rs_n = rup(c.n - 1, 256);
-    (void)Rs_m;
-    if (!make_map(&b.mapX, b.Xs, Kn, Rm, b.sX, bk, 128) || !make_map(&b.mapT, b.Ts, Km, Rn, b.sT, bk, b.bn) ||
-        !make_map(&b.mapSm, b.Sm, Km, rup(c.m - 1, 256), b.sSm, bk, 128) ||
-        !make_map(&b.mapSn, b.Sn, Kn, Rs_n, b.sSn, bk, b.bn)) {
+    if (!make_map(&b.mapX, b.Xs, Kn, Rm, b.sX, 64, 128) || !make_map(&b.mapT, b.Ts, Km, Rn, b.sT, 64, 128) ||
+        !make_map(&b.mapSm, b.Sm, Km, Rs_m, b.sSm, 64, 128) || !make_map(&b.mapSn, b.Sn, Kn, Rs_n, b.sSn, 64, 128) ||
+        !make_map(&b.mapX2, b.Xs, Kn, Rm, b.sX, 32, 128) || !make_map(&b.mapT2, b.Ts, Km, Rn, b.sT, 32, 256) ||
+        !make_map(&b.mapSm2, b.Sm, Km, Rs_m, b.sSm, 32, 128) ||
+        !make_map(&b.mapSn2, b.Sn, Kn, Rs_n, b.sSn, 32, 256)) {
       g_perr = "cuTensorMapEncodeTiled failed";
       return 4;
     }
@@ -755,6 +778,10 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
 }
 
 void precision_free(PrecisionPlan* pp) { delete pp; }
+
+void precision_set_tile(PrecisionPlan* pp, int width) { pp->tc_tile = (width == 128 || width == 256) ? width : 0; }
+const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp) { return pp->tile_choice; }
+void precision_reset_tile_choices(PrecisionPlan* pp) { pp->tile_choice.clear(); }
 
 int precision_set_wait_limit(PrecisionPlan* pp, double seconds) {
   if (!pp || !pp->wait_ns || !(seconds >= 0.0) || seconds > 60.0) return 7;
@@ -781,25 +808,121 @@ static T* upload(PrecisionPlan* pp, const std::vector<T>& v) {
   return p;
 }
 
-// One persistent launch over every tile of every descriptor, work items
-// sorted by K length (longest first) for balance across the SMs.
-static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& ds, cudaStream_t st) {
-  if (ds.empty()) return;
+// Work list of one launch group for output tiles 128 x bn: every tile of
+// every descriptor, sorted by K length (longest first) for balance across the
+// SMs.
+static std::vector<TcWork> tc_work(const std::vector<TcDesc>& ds, int bn) {
   std::vector<TcWork> wl;
-  double fl = 0.0;
   for (int i = 0; i < (int)ds.size(); i++) {
-    for (int t = 0; t < ds[i].tiles_m * ds[i].tiles_n; t++) wl.push_back({i, t});
-    const TcDesc& d = ds[i];
-    fl += 2.0 * d.M * (double)d.N * (double)(d.epi == TC_SPLIT_COL ? d.N : d.M);
+    const int tiles = ds[i].tiles_m * ((ds[i].N + bn - 1) / bn);
+    for (int t = 0; t < tiles; t++) wl.push_back({i, t});
   }
   std::stable_sort(wl.begin(), wl.end(), [&](const TcWork& x, const TcWork& y) { return ds[x.desc].Kp > ds[y.desc].Kp; });
+  return wl;
+}
+
+static void launch_tc(int bn, const TcDesc* dd, const TcWork* dw, int nw, int* status, const unsigned long long* wait_ns,
+                      cudaStream_t st) {
+  const int grid = std::min(nw, g_num_sms > 0 ? g_num_sms : 148);
+  if (bn == 256)
+    k_gemm_tc_persist<256><<<grid, kPThreads, tc_smem<256>(), st>>>(dd, dw, nw, status, wait_ns);
+  else
+    k_gemm_tc_persist<128><<<grid, kPThreads, tc_smem<128>(), st>>>(dd, dw, nw, status, wait_ns);
+}
+
+// Measured autotuner of the tensor-core GEMM's output tile (128 x 128 with K
+// blocks of 64, or 128 x 256 with K blocks of 32). A launch group is timed
+// once with each shape -- its outputs redirected to a scratch buffer, its
+// operands read where they lie, so no state changes -- and the faster shape
+// is kept, cached per process and device by the group's shape signature.
+// Both shapes issue the same slice products; only the order of the FP32
+// accumulation differs (K blocks of 32 against 64), which the refinement
+// sweep's FP64 residual absorbs.
+static std::mutex g_tc_mu;
+static std::map<std::string, int> g_tc_tuned;
+
+static std::string tc_signature(const std::vector<TcDesc>& ds) {
+  std::vector<std::string> parts;
+  for (auto& d : ds)
+    parts.push_back(std::to_string(d.M) + "x" + std::to_string(d.N) + "x" + std::to_string(d.Kp) + ":" +
+                    std::to_string(d.epi) + "/" + std::to_string(d.nprod));
+  std::sort(parts.begin(), parts.end());
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::string key = "dev" + std::to_string(dev) + "|";
+  for (auto& p : parts) key += p + ";";
+  return key;
+}
+
+static int tune_tc(PrecisionPlan* pp, const std::vector<TcDesc>& ds, cudaStream_t st) {
+  const std::string key = tc_signature(ds);
+  std::lock_guard<std::mutex> lk(g_tc_mu);
+  auto it = g_tc_tuned.find(key);
+  if (it != g_tc_tuned.end()) return it->second;
+  size_t need = 16;
+  for (auto& d : ds) {
+    if (d.epi == TC_SPLIT_COL || d.epi == TC_SCALE_SPLIT_ROW) need = std::max(need, (size_t)(3 * d.sC) * sizeof(bf16));
+    else need = std::max(need, (size_t)d.ldc * d.N * sizeof(double));
+  }
+  int best = 128;
+  void* scratch = nullptr;
+  TcDesc* dd = nullptr;
+  TcWork* dw = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<TcDesc> t = ds;
+  size_t maxw = 0;
+  for (int bn : {128, 256}) maxw = std::max(maxw, tc_work(ds, bn).size());
+  if (cudaMalloc(&scratch, need) == cudaSuccess && cudaMalloc(&dd, sizeof(TcDesc) * t.size()) == cudaSuccess &&
+      cudaMalloc(&dw, sizeof(TcWork) * maxw) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+      cudaEventCreate(&e1) == cudaSuccess) {
+    cudaMemsetAsync(scratch, 0, need, st);
+    for (auto& d : t) {
+      if (d.Cs) d.Cs = (bf16*)scratch;
+      if (d.C64) d.C64 = (double*)scratch;
+    }
+    cudaMemcpy(dd, t.data(), sizeof(TcDesc) * t.size(), cudaMemcpyHostToDevice);
+    float best_ms = 1e30f;
+    for (int bn : {128, 256}) {
+      const std::vector<TcWork> wl = tc_work(ds, bn);
+      cudaMemcpy(dw, wl.data(), sizeof(TcWork) * wl.size(), cudaMemcpyHostToDevice);
+      const int nw = (int)wl.size();
+      launch_tc(bn, dd, dw, nw, pp->status, pp->wait_ns, st);  // warm-up
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < 3; r++) launch_tc(bn, dd, dw, nw, pp->status, pp->wait_ns, st);
+      cudaEventRecord(e1, st);
+      float ms = 0.f;
+      if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
+          ms < best_ms) {
+        best_ms = ms;
+        best = bn;
+      }
+    }
+  }
+  cudaGetLastError();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (dw) cudaFree(dw);
+  if (dd) cudaFree(dd);
+  if (scratch) cudaFree(scratch);
+  g_tc_tuned[key] = best;
+  return best;
+}
+
+// One persistent launch over every tile of every descriptor, with the output
+// tile the handle's option or the autotuner chose.
+static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& ds, cudaStream_t st) {
+  if (ds.empty()) return;
+  const int bn = pp->tc_tile == 128 || pp->tc_tile == 256 ? pp->tc_tile : tune_tc(pp, ds, st);
+  pp->tile_choice.push_back(bn);
+  std::vector<TcWork> wl = tc_work(ds, bn);
+  double fl = 0.0;
+  for (auto& d : ds) fl += 2.0 * d.M * (double)d.N * (double)(d.epi == TC_SPLIT_COL ? d.N : d.M);
   TcDesc* dd = upload(pp, ds);
   TcWork* dw = upload(pp, wl);
-  int nw = (int)wl.size();
-  int grid = std::min(nw, g_num_sms > 0 ? g_num_sms : 148);
+  const int nw = (int)wl.size();
   int* status = pp->status;
   const unsigned long long* wait_ns = pp->wait_ns;
-  P.push_back({[=]() { k_gemm_tc_persist<<<grid, kPThreads, kPSmem, st>>>(dd, dw, nw, status, wait_ns); }, TAG_GEMM_TC, fl});
+  P.push_back({[=]() { launch_tc(bn, dd, dw, nw, status, wait_ns, st); }, TAG_GEMM_TC, fl});
 }
 
 static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all, cudaStream_t st) {
@@ -841,14 +964,16 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       }
       if (!(pass == 0 && r.presplit)) prep.push_back(pd);
       int M = c.m - 1, N = c.n - 1;
-      int tm = (M + 127) / 128, tn = (N + b.bn - 1) / b.bn;
+      int tm = (M + 127) / 128;
       TcDesc R{};  // T = X * S_n
       R.mapA = b.mapX; R.mapB = b.mapSn;
-      R.M = M; R.N = N; R.Kp = rup(N, 64); R.tiles_m = tm; R.tiles_n = tn; R.bn = b.bn;
+      R.mapA2 = b.mapX2; R.mapB2 = b.mapSn2;
+      R.M = M; R.N = N; R.Kp = rup(N, 64); R.tiles_m = tm;
       R.epi = TC_SPLIT_COL; R.Cs = b.Ts; R.sC = b.sT; R.ldcs = b.ldT;
       TcDesc L1{};  // U = f .* (S_m * T)
       L1.mapA = b.mapSm; L1.mapB = b.mapT;
-      L1.M = M; L1.N = N; L1.Kp = rup(M, 64); L1.tiles_m = tm; L1.tiles_n = tn; L1.bn = b.bn;
+      L1.mapA2 = b.mapSm2; L1.mapB2 = b.mapT2;
+      L1.M = M; L1.N = N; L1.Kp = rup(M, 64); L1.tiles_m = tm;
       L1.epi = TC_SCALE_SPLIT_ROW; L1.fkind = r.fkind; L1.Cs = b.Xs; L1.sC = b.sX; L1.ldcs = b.ldX;
       L1.lamx = b.lamx; L1.lamy = b.lamy; L1.norm = (float)c.norm;
       L1.nu = (float)(0.5 * c.dt / (c.delta * c.delta * std::pow(4.0, r.k - 1) * c.re));
@@ -899,27 +1024,28 @@ void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, co
       r.out = om;
       rq.push_back(r);
     }
-    LevelItem* d_it = upload(pp, it);
-    const std::vector<int2> bmv = block_map(cnt);
-    const int2* bm = upload(pp, bmv);
-    const int nbm = (int)bmv.size();
-    P.push_back({[=]() { launch_rhs(dcases, d_it, bm, nbm, 0, st); }, TAG_STENCIL, 0.0});
-    // b must be formed before omega_k is overwritten by x0: keep b in wd
-    std::vector<PrepDesc> bprep;
-    for (auto& r : rq) {
+    // b = norm*rhsA + (I - nu_k C^T C) omega_k is assembled once, in the same
+    // pass as the nonlinear term (k_rhs_split): FP64 copy in wd for the
+    // correction residual, BF16 slices for the first solve; b must be formed
+    // before omega_k is overwritten by x0
+    std::vector<RhsSplitDesc> sd;
+    std::vector<int2> tmap;
+    for (size_t q = 0; q < rq.size(); q++) {
+      SolveReq& r = rq[q];
       const DevCase& c = *r.hc;
-      PrepDesc pd = r.src;
-      pd.m = c.m; pd.n = c.n;
-      pd.Xs = pp->bufs[r.c].Xs; pd.sX = pp->bufs[r.c].sX; pd.ld = pp->bufs[r.c].ldX;
-      pd.out64 = c.wd;  // b
-      bprep.push_back(pd);
+      const CaseBufs& b = pp->bufs[r.c];
+      sd.push_back({c.norm, r.src.nu_om, c.wd, reinterpret_cast<uint16_t*>(b.Xs), b.sX, b.ldX});
+      const int tiles = ((c.m - 1 + 31) / 32) * ((c.n - 1 + 31) / 32);
+      for (int t = 0; t < tiles; t++) tmap.push_back(make_int2((int)q, t));
       r.src = PrepDesc{};
       r.src.src = c.wd; r.src.src_scale = 1.0;
       r.presplit = true;
     }
-    // b is assembled once (FP64 copy in wd for the correction residual, BF16
-    // slices for the first solve)
-    add_prep(pp, P, bprep, st);
+    LevelItem* d_it = upload(pp, it);
+    const RhsSplitDesc* d_sd = upload(pp, sd);
+    const int2* d_tm = upload(pp, tmap);
+    const int ntm = (int)tmap.size();
+    P.push_back({[=]() { launch_rhs_split(dcases, d_it, d_sd, d_tm, ntm, 0, st); }, TAG_STENCIL, 0.0});
     build_solves(pp, P, rq, st);
   }
 }
@@ -1004,7 +1130,9 @@ int precision_apply_op(PrecisionPlan* pp, int op, const DevCase* ds, const DevCa
   rq[0].fkind = op == 1 ? F_LAMINV : F_LAM1I_NORM;
   rq[0].src.src = s.vort; rq[0].src.src_scale = op == 1 ? 1.0 : 1.0;
   rq[0].out = s.omega;
+  const size_t nchoice = pp->tile_choice.size();
   build_solves(pp, P, rq, st);
+  pp->tile_choice.resize(nchoice);  // the step program's record stays as it was
   for (auto& e : P) e.fn();
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return 4;

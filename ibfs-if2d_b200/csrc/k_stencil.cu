@@ -2,6 +2,8 @@
 // of the IBFS advance. Each kernel follows the reference loop it replaces
 // (atchieu/ibfs-if2d src/operators.f90, cited per kernel); all arithmetic is
 // FP64. Grids are grouped: blockIdx.y selects a (case, level) item.
+#include <cuda_bf16.h>
+
 #include "ibfs_common.cuh"
 #include "ibfs_kernels.cuh"
 
@@ -48,14 +50,28 @@ __device__ __forceinline__ double uavg_at(const double* __restrict__ q, const do
   int a = uoff(i, j, m), b = uoff(i, j - 1, m);
   return 0.5 * (q[a] + q[b] + q0[a] + q0[b]);
 }
+// The same averages with q0 in closed form (u-faces u0, v-faces 0): the
+// reference's sums with the q0 terms in place, so the values are identical.
+__device__ __forceinline__ double vavg_c(const double* __restrict__ q, int i, int j, int m, int n) {
+  int a = voff(i, j, m, n), b = voff(i - 1, j, m, n);
+  return 0.5 * (q[a] + q[b] + 0.0 + 0.0);
+}
+__device__ __forceinline__ double uavg_c(const double* __restrict__ q, double u0, int i, int j, int m) {
+  int a = uoff(i, j, m), b = uoff(i, j - 1, m);
+  return 0.5 * (q[a] + q[b] + u0 + u0);
+}
 
-__device__ __forceinline__ void rhs_at(const DevCase& C, LevelItem it, int t, int first_step) {
+// The per-node values of the level update's right-hand side: returns rhsA =
+// con1*rhs + con2*rhs_old + rhsbc and stores rhs_old = rhs (operators.f90:112-133).
+template <bool Q0C>
+__device__ __forceinline__ double rhs_value(const DevCase& C, LevelItem it, int t, int first_step) {
   int m = C.m, n = C.n;
   int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
   int k = it.k;
   const double* om = C.omega + (size_t)(k - 1) * C.ns;
   const double* q = C.q + (size_t)(k - 1) * C.nq;
   const double* q0 = C.q0 + (size_t)(k - 1) * C.nq;
+  const double u0 = C.q0_u1 * (double)(1 << (k - 1));
   const double* bc = C.lastbc + (size_t)(k - 1) * C.nring;
   int bottom = 2 * (n + 1), top = 2 * (n + 1) + m + 1, right = n + 1;
   // omega extended with the ring along j (column i) and along i (row j)
@@ -69,11 +85,13 @@ __device__ __forceinline__ void rhs_at(const DevCase& C, LevelItem it, int t, in
     if (ii == m + 1) return bc[right + jj - 1];
     return om[nidx(ii, jj, m)];
   };
+  auto vavg = [&](int ii, int jj) -> double { return Q0C ? vavg_c(q, ii, jj, m, n) : vavg_at(q, q0, ii, jj, m, n); };
+  auto uavg = [&](int ii, int jj) -> double { return Q0C ? uavg_c(q, u0, ii, jj, m) : uavg_at(q, q0, ii, jj, m); };
   auto fqu = [&](int jj) -> double {  // fq(u(i,jj)), jj = 1..n
-    return 0.5 * (vavg_at(q, q0, i, jj + 1, m, n) * Wj(jj + 1) + vavg_at(q, q0, i, jj, m, n) * Wj(jj));
+    return 0.5 * (vavg(i, jj + 1) * Wj(jj + 1) + vavg(i, jj) * Wj(jj));
   };
   auto fqv = [&](int ii) -> double {  // fq(v(ii,j)), ii = 1..m
-    return -0.5 * (uavg_at(q, q0, ii + 1, j, m) * Wi(ii + 1, j) + uavg_at(q, q0, ii, j, m) * Wi(ii, j));
+    return -0.5 * (uavg(ii + 1, j) * Wi(ii + 1, j) + uavg(ii, j) * Wi(ii, j));
   };
   double rhs = fqv(i) - fqv(i - 1) - fqu(j) + fqu(j - 1);
 
@@ -97,8 +115,8 @@ __device__ __forceinline__ void rhs_at(const DevCase& C, LevelItem it, int t, in
   double del22 = C.delta * C.delta * (double)(1 << (2 * (k - 1)));
   double con1 = 1.5 * C.dt / del22 / C.norm;
   double con2 = -0.5 * C.dt / del22 / C.norm;
-  C.rhsA[t] = con1 * rhs + con2 * rold + rb;
   ro[t] = rhs;
+  return con1 * rhs + con2 * rold + rb;
 }
 
 // Grouped launches use a block map: block b covers elements
@@ -110,7 +128,95 @@ __global__ void __launch_bounds__(256) k_rhs(const DevCase* __restrict__ cases, 
   const LevelItem it = items[bm.x];
   const DevCase& C = cases[it.c];
   const int tend = min(C.ns, bm.y + kBlockElems);
-  for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) rhs_at(C, it, t, first_step);
+  if (C.q0_const) {
+    for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) C.rhsA[t] = rhs_value<true>(C, it, t, first_step);
+  } else {
+    for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) C.rhsA[t] = rhs_value<false>(C, it, t, first_step);
+  }
+}
+
+// Split-precision form: the level update's right-hand side assembled to the
+// solve's input in one pass over one 32 x 32 node tile per block,
+//   b = norm * rhsA + (omega_k - nu_k C^T C omega_k)
+// (the Crank-Nicolson form of operators.f90:126-130 with the explicit half of
+// the diffusion applied by the 5-point stencil), written as FP64 (the
+// refinement residual's right-hand side) and as three BF16 slices, row-major,
+// through a shared-memory transpose. rhs_old = rhs as in k_rhs; rhsA itself
+// is never stored.
+__device__ __forceinline__ double lap5_nodes(const double* __restrict__ x, int i, int j, int M, int N) {
+  double c = x[i + (size_t)j * M];
+  double s = 4.0 * c;
+  if (i > 0) s -= x[i - 1 + (size_t)j * M];
+  if (i + 1 < M) s -= x[i + 1 + (size_t)j * M];
+  if (j > 0) s -= x[i + (size_t)(j - 1) * M];
+  if (j + 1 < N) s -= x[i + (size_t)(j + 1) * M];
+  return s;
+}
+
+__device__ __forceinline__ void split3_bf16(double x, uint16_t& s0, uint16_t& s1, uint16_t& s2) {
+  __nv_bfloat16 a = __double2bfloat16(x);
+  double r = x - (double)__bfloat162float(a);
+  __nv_bfloat16 b = __double2bfloat16(r);
+  r = r - (double)__bfloat162float(b);
+  __nv_bfloat16 c = __double2bfloat16(r);
+  s0 = __bfloat16_as_ushort(a);
+  s1 = __bfloat16_as_ushort(b);
+  s2 = __bfloat16_as_ushort(c);
+}
+
+__global__ void __launch_bounds__(256) k_rhs_split(const DevCase* __restrict__ cases,
+                                                   const LevelItem* __restrict__ items,
+                                                   const RhsSplitDesc* __restrict__ sd,
+                                                   const int2* __restrict__ bmap, int first_step) {
+  const int2 bm = bmap[blockIdx.x];
+  const LevelItem it = items[bm.x];
+  const RhsSplitDesc& d = sd[bm.x];
+  const DevCase& C = cases[it.c];
+  const int M = C.m - 1, N = C.n - 1;
+  const int ti = (M + 31) / 32;
+  const int i0 = (bm.y % ti) * 32, j0 = (bm.y / ti) * 32;
+  const double* om = C.omega + (size_t)(it.k - 1) * C.ns;
+  __shared__ double tile[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  const bool q0c = C.q0_const != 0;
+  for (int jj = ty; jj < 32; jj += 8) {
+    const int i = i0 + tx, j = j0 + jj;
+    double v = 0.0;
+    if (i < M && j < N) {
+      const int t = i + j * M;
+      const double rA = q0c ? rhs_value<true>(C, it, t, first_step) : rhs_value<false>(C, it, t, first_step);
+      v = d.scale * rA;
+      v = v + (om[t] - d.nu * lap5_nodes(om, i, j, M, N));
+      d.b64[t] = v;
+    }
+    tile[jj][tx] = v;
+  }
+  __syncthreads();
+  const int ii = threadIdx.x >> 3, g = threadIdx.x & 7;  // row ii, columns 4g .. 4g+3
+  const int i = i0 + ii, j = j0 + 4 * g;
+  if (i < M && j < N) {
+    uint16_t a[4], b[4], c[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) split3_bf16(tile[4 * g + e][ii], a[e], b[e], c[e]);
+    // row stride and slice stride are multiples of 64 elements: 8-byte aligned
+    // groups; columns >= N of the last group are zero (the K padding)
+    uint16_t* o = d.Xs + (size_t)i * d.ld + j;
+    auto st4 = [](uint16_t* p, const uint16_t* w) {
+      uint2 u;
+      u.x = (uint32_t)w[0] | ((uint32_t)w[1] << 16);
+      u.y = (uint32_t)w[2] | ((uint32_t)w[3] << 16);
+      *reinterpret_cast<uint2*>(p) = u;
+    };
+    st4(o, a);
+    st4(o + d.sX, b);
+    st4(o + 2 * d.sX, c);
+  }
+}
+
+void launch_rhs_split(const DevCase* cases, const LevelItem* items, const RhsSplitDesc* sd, const int2* bmap,
+                      int nblocks, int first, cudaStream_t st) {
+  if (nblocks == 0) return;
+  k_rhs_split<<<nblocks, 256, 0, st>>>(cases, items, sd, bmap, first);
 }
 
 // ---------------------------------------------------------------------------

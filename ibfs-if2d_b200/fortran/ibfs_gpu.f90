@@ -36,6 +36,7 @@ MODULE ibfs_gpu
      REAL(C_DOUBLE) :: pitch_amp_deg, pitch_freq, pivot_x, pivot_y
      INTEGER(C_INT) :: tile_cfg
      INTEGER(C_INT) :: cg_precond
+     INTEGER(C_INT) :: tc_tile
   END TYPE ibfs_options_c
 
   INTERFACE

@@ -249,11 +249,11 @@ int main(int argc, char** argv) {
                 "\"re\": %.17g, \"cgtol\": %.17g, \"cg_max_iter\": %d, \"unif_flow\": %d, \"len\": %.17g, "
                 "\"offsetx\": %.17g, \"offsety\": %.17g, \"mgridlev\": %d, \"make_vortex\": %d, "
                 "\"stationary\": %d, \"precision\": %d, \"cg_relative\": %d, \"motion_kind\": %d, "
-                "\"tile_cfg\": %d, \"cg_precond\": %d, \"nb\": %d, \"x0\": %.17g, \"y0\": %.17g, \"xsum\": %.17g, \"ysum\": %.17g, "
+                "\"tile_cfg\": %d, \"cg_precond\": %d, \"tc_tile\": %d, \"nb\": %d, \"x0\": %.17g, \"y0\": %.17g, \"xsum\": %.17g, \"ysum\": %.17g, "
                 "\"n_act\": %d, \"n_act_pt\": %d, \"chd_ok\": %d, \"var_sums\": [",
                 p.istart, p.istop, p.isave, p.m, p.n, p.dt, p.re, p.cgtol, p.cg_max_iter, p.unif_flow, p.len,
                 p.offsetx, p.offsety, p.mgridlev, p.make_vortex, p.stationary, opt.precision, opt.cg_relative,
-                opt.motion_kind, opt.tile_cfg, opt.cg_precond, nb, nb ? geo.x[0] : 0.0, nb ? geo.y[0] : 0.0,
+                opt.motion_kind, opt.tile_cfg, opt.cg_precond, opt.tc_tile, nb, nb ? geo.x[0] : 0.0, nb ? geo.y[0] : 0.0,
                 [&] { double t = 0.0; for (double v : geo.x) t += v; return t; }(),
                 [&] { double t = 0.0; for (double v : geo.y) t += v; return t; }(), n_act, n_act_pt, chd_ok);
     for (size_t i = 0; i < var_sums.size(); i++) std::printf("%s%.17g", i ? ", " : "", var_sums[i]);

@@ -26,7 +26,7 @@ EXPORTS = [
     "ibfs_advance", "ibfs_advance_n", "ibfs_batch_advance", "ibfs_output_offset", "ibfs_output_stride", "ibfs_apply_op",
     "ibfs_last_timing", "ibfs_kernels_per_step", "ibfs_profile_step", "ibfs_dst2d_noalloc",
     "ibfs_last_cg_iterations", "ibfs_adjoint_run", "ibfs_adjoint_pitch_run", "ibfs_vertex_fields",
-    "ibfs_set_actuators", "ibfs_set_wait_limit",
+    "ibfs_set_actuators", "ibfs_set_wait_limit", "ibfs_gemm_tiles",
     "ibfs_last_error",
 ]
 
@@ -48,7 +48,7 @@ class Options(ctypes.Structure):
         ("precision", ctypes.c_int), ("cg_relative", ctypes.c_int), ("motion_kind", ctypes.c_int),
         ("pitch_amp_deg", ctypes.c_double), ("pitch_freq", ctypes.c_double),
         ("pivot_x", ctypes.c_double), ("pivot_y", ctypes.c_double), ("tile_cfg", ctypes.c_int),
-        ("cg_precond", ctypes.c_int),
+        ("cg_precond", ctypes.c_int), ("tc_tile", ctypes.c_int),
     ]
 
 
@@ -98,6 +98,7 @@ def lib():
         L.ibfs_set_actuators.argtypes = [vp, ctypes.c_int, ctypes.c_int, _IP, _DP, _DP, _DP, _DP]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
         L.ibfs_set_wait_limit.argtypes = [vp, ctypes.c_double]
+        L.ibfs_gemm_tiles.argtypes = [vp, _IP, ctypes.c_int]
         L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
         L.ibfs_last_error.argtypes = [vp]
@@ -120,9 +121,9 @@ def make_params(m, n, dt, re, mgridlev, len_=4.0, offsetx=2.0, offsety=2.0, stat
 
 
 def make_options(precision=0, cg_relative=0, motion_kind=0, pitch_amp_deg=0.0, pitch_freq=0.0,
-                 pivot_x=0.0, pivot_y=0.0, tile_cfg=-1, cg_precond=0):
+                 pivot_x=0.0, pivot_y=0.0, tile_cfg=-1, cg_precond=0, tc_tile=0):
     return Options(precision, cg_relative, motion_kind, pitch_amp_deg, pitch_freq, pivot_x, pivot_y,
-                   tile_cfg, cg_precond)
+                   tile_cfg, cg_precond, tc_tile)
 
 
 class Solver:
@@ -312,6 +313,13 @@ class Solver:
 
     def kernels_per_step(self):
         return lib().ibfs_kernels_per_step(self.h)
+
+    def gemm_tiles(self):
+        """Output tile widths of the tensor-core GEMM launch groups of the step."""
+        n = lib().ibfs_gemm_tiles(self.h, None, 0)
+        out = np.zeros(max(n, 1), dtype=np.int32)
+        lib().ibfs_gemm_tiles(self.h, out.ctypes.data_as(_IP), n)
+        return [int(x) for x in out[:n]]
 
     TAGS = ("stencil", "gemm_f64", "gemm_tc", "chol", "split")
 

@@ -69,6 +69,10 @@ typedef struct {
                           applied as z = Q L_k^-T L_k^-1 Q^T r with Q the remaining
                           rotation of each point's (fx, fy); a body that does not move
                           has one slot. Same stop rule on the true residual        */
+  int tc_tile;         /* split-precision form: output tile width of the tensor-core GEMM,
+                          128 (K blocks of 64) or 256 (K blocks of 32); 0 = the measured
+                          autotuner picks per launch group. Taken from the first case of
+                          a batch                                                  */
 } ibfs_options_c;
 
 typedef struct ibfs_handle ibfs_handle;
@@ -167,6 +171,12 @@ int ibfs_last_timing(const ibfs_handle* h, double* ms);
 /* Number of kernel launches in one captured step graph (no reference
  * counterpart; reports the launch structure of the advance). */
 int ibfs_kernels_per_step(const ibfs_handle* h);
+
+/* Output tile widths (128 or 256) of the split-precision form's tensor-core
+ * GEMM launch groups of the step program, in launch order: writes up to max
+ * of them to widths (may be NULL) and returns how many there are (0 for a
+ * plain FP64 handle). No reference counterpart (reports the tuner's choice). */
+int ibfs_gemm_tiles(const ibfs_handle* h, int* widths, int max);
 
 /* Discrete adjoint of nsteps advances (no reference counterpart; the
  * reference has no derivatives). For a single-case handle, stationary body,
