@@ -662,6 +662,7 @@ def run_ours(args):
             "roofline": roof, "roofline_step_hbm": roof_step, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": kern * args.steps, "kernels_per_step": kern, "profile_step": prof,
             "gemm_tiles": {str(w): g.gemm_tiles().count(w) for w in (128, 256)},
+            "gemm_tiles": {str(w): g.gemm_tiles().count(w) for w in (128, 256)},
             "clocks": cs.summary(), "impl": "ours",
         }
         out.update(extras)

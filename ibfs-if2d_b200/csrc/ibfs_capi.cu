@@ -177,12 +177,14 @@ static double* cos_table(ibfs_handle* h, int m) {
 
 // ---------------------------------------------------------------------------
 // Tile autotuner of the FP64 transform GEMMs. A launch group (the GEMMs of one
-// step-program entry) is timed once with each of the four tile shapes --
-// its outputs redirected to a scratch buffer, its inputs read where they lie,
-// so no state changes -- and the fastest shape is kept. Results are cached
-// per process and device by the group's shape signature, so handles of the
-// same sizes tune once. The tile shape does not change the order of any
-// output's K sum: every shape gives bit-identical results.
+// step-program entry) is timed once with each tile configuration -- the four
+// unsplit shapes and the three split-K cluster variants -- its outputs
+// redirected to a scratch buffer, its inputs read where they lie, so no state
+// changes, and the fastest configuration is kept. Results are cached per
+// process and device by the group's shape signature, so handles of the same
+// sizes tune once. The unsplit shapes do not change the order of any output's
+// K sum (bit-identical results); the split variants add the K partial sums in
+// a fixed order (deterministic, equal to round-off).
 static std::mutex g_tune_mu;
 static std::map<std::string, int> g_tuned;
 
@@ -224,7 +226,7 @@ static int tune_gemm(const std::vector<GemmDesc>& ds, bool dual, cudaStream_t st
     }
     cudaMemcpy(dd, t.data(), sizeof(GemmDesc) * t.size(), cudaMemcpyHostToDevice);
     float best_ms = 1e30f;
-    for (int cfg = 0; cfg < 4; cfg++) {
+    for (int cfg = 0; cfg < kGemmF64Cfgs; cfg++) {
       int mt = 0;
       for (auto& d : t) mt = std::max(mt, gemm_tiles(d.M, d.N, cfg));
       launch_gemm_f64(dd, (int)t.size(), mt, cfg, dual, st);  // warm-up
@@ -261,7 +263,7 @@ struct ProgBuilder {
   void add(std::function<void()> fn, int tag = TAG_STENCIL, double flops = 0.0) { P.push_back({fn, tag, flops}); }
   void gemm(std::vector<GemmDesc> ds, bool dual) {
     if (ds.empty()) return;
-    const int cfg = h->tile_cfg >= 0 ? h->tile_cfg : tune_gemm(ds, dual, h->st);
+    const int cfg = h->tile_cfg >= 0 && h->tile_cfg < kGemmF64Cfgs ? h->tile_cfg : tune_gemm(ds, dual, h->st);
     int mt = 0;
     for (auto& d : ds) mt = std::max(mt, gemm_tiles(d.M, d.N, cfg));
     GemmDesc* dd = dupload(h, ds);

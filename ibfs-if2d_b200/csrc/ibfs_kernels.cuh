@@ -47,6 +47,9 @@ struct GemmDesc {
   double dt, re, del22, norm;
 };
 
+// tile_cfg 0..3: unsplit tiles (bit-identical results); 4..6: split-K over a
+// cluster of 2 or 4 blocks (kGemmF64Cfgs configurations in all)
+constexpr int kGemmF64Cfgs = 7;
 void launch_gemm_f64(const GemmDesc* d_descs, int ndesc, int max_tiles, int tile_cfg, bool dual, cudaStream_t st);
 int gemm_tiles(int M, int N, int tile_cfg);
 void gemm_f64_init();

@@ -10,22 +10,36 @@
 // (BM/16)x(BN/16) micro-tile on a strided lattice (conflict-free shared loads),
 // double-buffered shared memory with register prefetch. Grouped: blockIdx.y
 // selects a GemmDesc, blockIdx.x a tile of it.
+//
+// Split-K variants (SPLIT = 2 or 4) fill the machine when a launch group has
+// few tiles (one case's 399^2 or 511^2 transform has 49-169 tiles for 148
+// SMs): the SPLIT thread blocks of a cluster share one output tile, each
+// summing a contiguous share of K; rank 0 adds the other ranks' partial tiles
+// from their shared memory (distributed shared memory) in rank order, then
+// applies the epilogue. The result is deterministic; it differs from the
+// unsplit sum only in the order of the K partial sums.
+#include <cooperative_groups.h>
+
 #include <mutex>
 
 #include "ibfs_common.cuh"
 #include "ibfs_kernels.cuh"
 
+namespace cg = cooperative_groups;
+
 namespace ibfs {
 
 constexpr int kBK = 16;
 
-template <int BM, int BN, bool DUAL>
+template <int BM, int BN, bool DUAL, int SPLIT>
 __global__ void __launch_bounds__(256) k_gemm_f64(const GemmDesc* __restrict__ descs) {
   const GemmDesc& d = descs[blockIdx.y];
   const int tiles_m = (d.M + BM - 1) / BM;
   const int tiles_n = (d.N + BN - 1) / BN;
-  if ((int)blockIdx.x >= tiles_m * tiles_n) return;
-  const int m0 = (blockIdx.x % tiles_m) * BM, n0 = (blockIdx.x / tiles_m) * BN;
+  const int tile = (int)blockIdx.x / SPLIT, rank = (int)blockIdx.x % SPLIT;
+  // a cluster's blocks share a tile; all of them (or none) pass this test
+  if (tile >= tiles_m * tiles_n) return;
+  const int m0 = (tile % tiles_m) * BM, n0 = (tile / tiles_m) * BN;
   constexpr int TM = BM / 16, TN = BN / 16;
   constexpr int A_PER = BM * kBK / 256, B_PER = kBK * BN / 256;
   constexpr int LDB = BN + 1;
@@ -94,12 +108,18 @@ __global__ void __launch_bounds__(256) k_gemm_f64(const GemmDesc* __restrict__ d
     }
   };
 
-  const int nk = (K + kBK - 1) / kBK;
-  load(0);
-  store(0);
+  // this block's K blocks: all of them, or a contiguous share of the split
+  const int nk_all = (K + kBK - 1) / kBK;
+  const int per = (nk_all + SPLIT - 1) / SPLIT;
+  const int kt0 = SPLIT > 1 ? min(nk_all, rank * per) : 0;
+  const int nk = SPLIT > 1 ? min(nk_all, kt0 + per) : nk_all;
+  if (kt0 < nk) {
+    load(kt0 * kBK);
+    store(0);
+  }
   __syncthreads();
-  for (int kt = 0; kt < nk; kt++) {
-    const int buf = kt & 1;
+  for (int kt = kt0; kt < nk; kt++) {
+    const int buf = (kt - kt0) & 1;
     if (kt + 1 < nk) load((kt + 1) * kBK);
     const double* as = As + buf * kBK * BM;
     const double* bs = Bs + buf * kBK * LDB;
@@ -126,6 +146,37 @@ __global__ void __launch_bounds__(256) k_gemm_f64(const GemmDesc* __restrict__ d
     }
     if (kt + 1 < nk) store(buf ^ 1);
     __syncthreads();
+  }
+
+  if (SPLIT > 1) {
+    // partial tiles through distributed shared memory, summed by rank 0 in
+    // rank order (the main loop's last __syncthreads freed the operand tiles)
+    double* part = smem;  // [TM*TN (x2 for DUAL)][256], thread-major per element
+    constexpr int NP = TM * TN;
+#pragma unroll
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TN; b++) {
+        part[(a * TN + b) * 256 + tid] = acc[a][b];
+        if (DUAL) part[(NP + a * TN + b) * 256 + tid] = acc2[DUAL ? a : 0][DUAL ? b : 0];
+      }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    if (rank == 0) {
+#pragma unroll 1
+      for (int r = 1; r < SPLIT; r++) {
+        const double* rp = cl.map_shared_rank(part, r);
+#pragma unroll
+        for (int a = 0; a < TM; a++)
+#pragma unroll
+          for (int b = 0; b < TN; b++) {
+            acc[a][b] += rp[(a * TN + b) * 256 + tid];
+            if (DUAL) acc2[DUAL ? a : 0][DUAL ? b : 0] += rp[(NP + a * TN + b) * 256 + tid];
+          }
+      }
+    }
+    cl.sync();  // the other ranks keep their shared memory until rank 0 has read it
+    if (rank != 0) return;
   }
 
   // epilogue
@@ -173,16 +224,27 @@ __global__ void __launch_bounds__(256) k_gemm_f64(const GemmDesc* __restrict__ d
   }
 }
 
-template <int BM, int BN, bool DUAL>
+template <int BM, int BN, bool DUAL, int SPLIT>
 static size_t smem_bytes() {
-  return sizeof(double) * (2 * kBK * BM + 2 * kBK * (BN + 1) * (DUAL ? 2 : 1));
+  const size_t ops = 2 * kBK * BM + 2 * kBK * (BN + 1) * (DUAL ? 2 : 1);
+  const size_t part = SPLIT > 1 ? (size_t)BM * BN * (DUAL ? 2 : 1) : 0;  // partial tiles of the split
+  return sizeof(double) * (ops > part ? ops : part);
 }
 
-template <int BM, int BN, bool DUAL>
+template <int BM, int BN, bool DUAL, int SPLIT>
 static void set_attr() {
-  cudaFuncSetAttribute(k_gemm_f64<BM, BN, DUAL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem_bytes<BM, BN, DUAL>());
+  cudaFuncSetAttribute(k_gemm_f64<BM, BN, DUAL, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem_bytes<BM, BN, DUAL, SPLIT>());
 }
+
+// Tile configurations: 0 64x64, 1 32x32, 2 64x32, 3 32x64 (unsplit; all four
+// give bit-identical results), 4 32x32 split in 2 along K, 5 64x64 split in 4,
+// 6 32x32 split in 4.
+struct F64Cfg {
+  int bm, bn, split;
+};
+static const F64Cfg kF64Cfg[kGemmF64Cfgs] = {{64, 64, 1}, {32, 32, 1}, {64, 32, 1}, {32, 64, 1},
+                                             {32, 32, 2}, {64, 64, 4}, {32, 32, 4}};
 
 // Raise the dynamic shared-memory limit of every instantiation (once per
 // process, before any stream capture; handles may be created from several
@@ -190,33 +252,54 @@ static void set_attr() {
 void gemm_f64_init() {
   static std::once_flag once;
   std::call_once(once, []() {
-    set_attr<64, 64, true>(); set_attr<64, 64, false>();
-    set_attr<32, 32, true>(); set_attr<32, 32, false>();
-    set_attr<64, 32, true>(); set_attr<64, 32, false>();
-    set_attr<32, 64, true>(); set_attr<32, 64, false>();
+    set_attr<64, 64, true, 1>(); set_attr<64, 64, false, 1>();
+    set_attr<32, 32, true, 1>(); set_attr<32, 32, false, 1>();
+    set_attr<64, 32, true, 1>(); set_attr<64, 32, false, 1>();
+    set_attr<32, 64, true, 1>(); set_attr<32, 64, false, 1>();
+    set_attr<32, 32, true, 2>(); set_attr<32, 32, false, 2>();
+    set_attr<64, 64, true, 4>(); set_attr<64, 64, false, 4>();
+    set_attr<32, 32, true, 4>(); set_attr<32, 32, false, 4>();
   });
 }
 
-template <int BM, int BN, bool DUAL>
+template <int BM, int BN, bool DUAL, int SPLIT>
 static void launch_cfg(const GemmDesc* d, int ndesc, int max_tiles, cudaStream_t st) {
-  size_t sm = smem_bytes<BM, BN, DUAL>();
-  dim3 g(max_tiles, ndesc);
-  k_gemm_f64<BM, BN, DUAL><<<g, 256, sm, st>>>(d);
+  const size_t sm = smem_bytes<BM, BN, DUAL, SPLIT>();
+  dim3 g(max_tiles * SPLIT, ndesc);
+  if (SPLIT == 1) {
+    k_gemm_f64<BM, BN, DUAL, SPLIT><<<g, 256, sm, st>>>(d);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = SPLIT;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_gemm_f64<BM, BN, DUAL, SPLIT>, d);
 }
 
 int gemm_tiles(int M, int N, int cfg) {
-  int bm = (cfg == 0 || cfg == 2) ? 64 : 32;
-  int bn = (cfg == 0 || cfg == 3) ? 64 : 32;
-  return ((M + bm - 1) / bm) * ((N + bn - 1) / bn);
+  const F64Cfg& c = kF64Cfg[cfg < 0 || cfg >= kGemmF64Cfgs ? 0 : cfg];
+  return ((M + c.bm - 1) / c.bm) * ((N + c.bn - 1) / c.bn);
 }
 
 void launch_gemm_f64(const GemmDesc* d, int ndesc, int max_tiles, int cfg, bool dual, cudaStream_t st) {
   if (ndesc == 0) return;
   switch (cfg) {
-    case 0: dual ? launch_cfg<64, 64, true>(d, ndesc, max_tiles, st) : launch_cfg<64, 64, false>(d, ndesc, max_tiles, st); break;
-    case 1: dual ? launch_cfg<32, 32, true>(d, ndesc, max_tiles, st) : launch_cfg<32, 32, false>(d, ndesc, max_tiles, st); break;
-    case 2: dual ? launch_cfg<64, 32, true>(d, ndesc, max_tiles, st) : launch_cfg<64, 32, false>(d, ndesc, max_tiles, st); break;
-    default: dual ? launch_cfg<32, 64, true>(d, ndesc, max_tiles, st) : launch_cfg<32, 64, false>(d, ndesc, max_tiles, st); break;
+    case 0: dual ? launch_cfg<64, 64, true, 1>(d, ndesc, max_tiles, st) : launch_cfg<64, 64, false, 1>(d, ndesc, max_tiles, st); break;
+    case 1: dual ? launch_cfg<32, 32, true, 1>(d, ndesc, max_tiles, st) : launch_cfg<32, 32, false, 1>(d, ndesc, max_tiles, st); break;
+    case 2: dual ? launch_cfg<64, 32, true, 1>(d, ndesc, max_tiles, st) : launch_cfg<64, 32, false, 1>(d, ndesc, max_tiles, st); break;
+    case 3: dual ? launch_cfg<32, 64, true, 1>(d, ndesc, max_tiles, st) : launch_cfg<32, 64, false, 1>(d, ndesc, max_tiles, st); break;
+    case 4: dual ? launch_cfg<32, 32, true, 2>(d, ndesc, max_tiles, st) : launch_cfg<32, 32, false, 2>(d, ndesc, max_tiles, st); break;
+    case 5: dual ? launch_cfg<64, 64, true, 4>(d, ndesc, max_tiles, st) : launch_cfg<64, 64, false, 4>(d, ndesc, max_tiles, st); break;
+    default: dual ? launch_cfg<32, 32, true, 4>(d, ndesc, max_tiles, st) : launch_cfg<32, 32, false, 4>(d, ndesc, max_tiles, st); break;
   }
 }
 

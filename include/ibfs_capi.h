@@ -60,7 +60,10 @@ typedef struct {
                           grid.f90:523-576); 1: rigid pitching about (pivot_x,pivot_y),
                           alpha(t) = amp*sin(2 pi f t), points move, reg rebuilt        */
   double pitch_amp_deg, pitch_freq, pivot_x, pivot_y;
-  int tile_cfg;        /* FP64 transform tile shape 0..3; -1 = the measured autotuner  */
+  int tile_cfg;        /* FP64 transform tile: 0..3 the unsplit shapes 64x64, 32x32,
+                          64x32, 32x64 (bit-identical results); 4..6 split-K over a
+                          cluster (32x32 in 2, 64x64 in 4, 32x32 in 4); -1 = the
+                          measured autotuner                                        */
   int cg_precond;      /* CG cases: 0 = cjgr as in the reference (unpreconditioned);
                           1 = preconditioned CG: the force operator factored with the
                           body turned by the grid angle nearest the step's pitch
@@ -269,10 +272,10 @@ int ibfs_dst2d_noalloc(const double* d_in, double* d_out, int m, int n, void* st
  * tensor memory and return; the advance then returns IBFS_ERR_TIMEOUT with
  * the role, block and pipeline step of the first wait that gave up, and the
  * handle's state is undefined (destroy it). A limit of 0 makes every wait
- * that does not succeed at once give up: it exercises this path (the
- * reference's counterpart is none; its waits cannot time out). The value is
- * read by the kernel from device memory, so it applies to captured step
- * graphs too. */
+ * that does not succeed at once give up, which exercises this path. The
+ * value is read by the kernel from device memory, so it applies to captured
+ * step graphs too. No reference counterpart (the reference has no device
+ * waits). */
 int ibfs_set_wait_limit(ibfs_handle* h, double seconds);
 
 /* Message of the last error on this handle (or of the last failed create). */
