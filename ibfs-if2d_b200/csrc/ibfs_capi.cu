@@ -177,14 +177,14 @@ static double* cos_table(ibfs_handle* h, int m) {
 
 // ---------------------------------------------------------------------------
 // Tile autotuner of the FP64 transform GEMMs. A launch group (the GEMMs of one
-// step-program entry) is timed once with each tile configuration -- the four
-// unsplit shapes and the three split-K cluster variants -- its outputs
-// redirected to a scratch buffer, its inputs read where they lie, so no state
-// changes, and the fastest configuration is kept. Results are cached per
-// process and device by the group's shape signature, so handles of the same
-// sizes tune once. The unsplit shapes do not change the order of any output's
-// K sum (bit-identical results); the split variants add the K partial sums in
-// a fixed order (deterministic, equal to round-off).
+// step-program entry) with enough tiles to fill the SMs is timed once with each
+// of the four unsplit tile shapes -- its outputs redirected to a scratch
+// buffer, its inputs read where they lie, so no state changes -- and the
+// fastest shape is kept. Results are cached per process and device by the
+// group's shape signature, so handles of the same sizes tune once. The
+// unsplit shapes do not change the order of any output's K sum: they give
+// bit-identical results. Groups with few tiles use a split-K cluster
+// variant fixed by their tile count (tune_gemm).
 static std::mutex g_tune_mu;
 static std::map<std::string, int> g_tuned;
 
@@ -200,7 +200,26 @@ static std::string gemm_signature(const std::vector<GemmDesc>& ds, bool dual) {
   return key;
 }
 
+static int num_sms() {
+  static int sms = [] {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    return n;
+  }();
+  return sms;
+}
+
 static int tune_gemm(const std::vector<GemmDesc>& ds, bool dual, cudaStream_t st) {
+  // A group with few 32x32 tiles (one or a few cases) leaves SMs idle: it gets
+  // a split-K cluster configuration, chosen by the tile count alone and never
+  // by timing, so that a group shape gets the same configuration -- the same
+  // summation order -- in every process and in every grouping of the same
+  // cases. Larger groups are timed over the unsplit shapes only, which give
+  // bit-identical results, so timing noise never changes a result.
+  long tiles32 = 0;
+  for (auto& d : ds) tiles32 += gemm_tiles(d.M, d.N, 1);
+  if (tiles32 < 2L * num_sms()) return tiles32 >= num_sms() / 2 ? 4 : 6;
   const int fallback = [&] {
     long tiles64 = 0;
     for (auto& d : ds) tiles64 += gemm_tiles(d.M, d.N, 0);
@@ -226,7 +245,7 @@ static int tune_gemm(const std::vector<GemmDesc>& ds, bool dual, cudaStream_t st
     }
     cudaMemcpy(dd, t.data(), sizeof(GemmDesc) * t.size(), cudaMemcpyHostToDevice);
     float best_ms = 1e30f;
-    for (int cfg = 0; cfg < kGemmF64Cfgs; cfg++) {
+    for (int cfg = 0; cfg < 4; cfg++) {
       int mt = 0;
       for (auto& d : t) mt = std::max(mt, gemm_tiles(d.M, d.N, cfg));
       launch_gemm_f64(dd, (int)t.size(), mt, cfg, dual, st);  // warm-up
@@ -1080,6 +1099,7 @@ static int finish_create(ibfs_handle* h) {
     });
     if (rc) return fail(rc, precision_error());
     precision_set_tile(h->prec, h->cases[0].o.tc_tile);
+    precision_set_refine_slices(h->prec, h->cases[0].o.refine_slices);
   }
   build_step_program(h);
   IBFS_CUDA_CHECK(cudaDeviceSynchronize());

@@ -21,6 +21,9 @@ void precision_free(PrecisionPlan* pp);
 int precision_set_wait_limit(PrecisionPlan* pp, double seconds);
 // Output tile width of the tensor-core GEMM: 128, 256, or 0 for the autotuner.
 void precision_set_tile(PrecisionPlan* pp, int width);
+// Slices per operand of the refinement sweep's correction solve: 3 (six
+// products) or 2 (three products).
+void precision_set_refine_slices(PrecisionPlan* pp, int slices);
 // Widths chosen for the GEMM launch groups built since the last reset.
 const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp);
 void precision_reset_tile_choices(PrecisionPlan* pp);

@@ -70,7 +70,7 @@ constexpr uint64_t kDrainLimitNs = 1000000000ull;
 
 // Bounded wait for the phase with the given parity (try_wait may suspend the
 // thread between polls); false once lim ns have passed since the first
-// failed poll.
+// failed poll (with lim = 0: at the second failed poll).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t lim) {
   uint64_t t0 = 0;
   for (;;) {
@@ -85,7 +85,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_
     if (done) return true;
     const uint64_t t = global_ns();  // the clock is read only once a poll has failed
     if (t0 == 0) t0 = t;
-    else if (t - t0 > lim) return false;
+    else if (t - t0 >= lim) return false;
   }
 }
 
@@ -107,7 +107,7 @@ __device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity, uint64_
     if ((it & 255) == 255) {  // no clock read on the fast path
       const uint64_t t = global_ns();
       if (t0 == 0) t0 = t;
-      else if (t - t0 > lim) return false;
+      else if (t - t0 >= lim) return false;
     }
   }
 }
@@ -633,6 +633,7 @@ struct PrecisionPlan {
   int* status = nullptr;
   unsigned long long* wait_ns = nullptr;  // limit of the GEMM's waits, ns (device word)
   int tc_tile = 0;                        // output tile width: 0 = the measured autotuner, 128 or 256
+  int refine_slices = 3;                  // slices per operand of the correction solve (3 or 2)
   std::vector<int> tile_choice;           // width used by each GEMM launch group, in build order
   Alloc alloc;
 };
@@ -780,6 +781,7 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
 void precision_free(PrecisionPlan* pp) { delete pp; }
 
 void precision_set_tile(PrecisionPlan* pp, int width) { pp->tc_tile = (width == 128 || width == 256) ? width : 0; }
+void precision_set_refine_slices(PrecisionPlan* pp, int slices) { pp->refine_slices = slices == 2 ? 2 : 3; }
 const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp) { return pp->tile_choice; }
 void precision_reset_tile_choices(PrecisionPlan* pp) { pp->tile_choice.clear(); }
 
@@ -980,10 +982,11 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       TcDesc L2 = L1;  // x = S_m * T'
       L2.epi = pass == 0 ? TC_F64_STORE : TC_F64_ADD;
       L2.C64 = r.out; L2.ldc = M;
-      // the correction solve acts on a residual already ~1e-6 of the data:
-      // two slices per operand (three products, ~1e-5) keep the refined error
-      // at ~1e-11 while halving the work of that pass
-      int np = pass == 0 ? 6 : 3;
+      // the correction solve acts on a residual already ~1e-6 of the data;
+      // with three slices per operand (six products) its own error is set by
+      // the FP32 accumulation (~1e-6), with two (three products) by the
+      // slices' 16 significant bits (~1e-5), ten times larger in the result
+      int np = pass == 0 ? 6 : (pp->refine_slices == 2 ? 3 : 6);
       R.nprod = np;
       L1.nprod = np;
       L2.nprod = np;

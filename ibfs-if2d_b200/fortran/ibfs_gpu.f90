@@ -37,6 +37,7 @@ MODULE ibfs_gpu
      INTEGER(C_INT) :: tile_cfg
      INTEGER(C_INT) :: cg_precond
      INTEGER(C_INT) :: tc_tile
+     INTEGER(C_INT) :: refine_slices
   END TYPE ibfs_options_c
 
   INTERFACE

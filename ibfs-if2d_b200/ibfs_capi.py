@@ -48,7 +48,7 @@ class Options(ctypes.Structure):
         ("precision", ctypes.c_int), ("cg_relative", ctypes.c_int), ("motion_kind", ctypes.c_int),
         ("pitch_amp_deg", ctypes.c_double), ("pitch_freq", ctypes.c_double),
         ("pivot_x", ctypes.c_double), ("pivot_y", ctypes.c_double), ("tile_cfg", ctypes.c_int),
-        ("cg_precond", ctypes.c_int), ("tc_tile", ctypes.c_int),
+        ("cg_precond", ctypes.c_int), ("tc_tile", ctypes.c_int), ("refine_slices", ctypes.c_int),
     ]
 
 
@@ -121,9 +121,9 @@ def make_params(m, n, dt, re, mgridlev, len_=4.0, offsetx=2.0, offsety=2.0, stat
 
 
 def make_options(precision=0, cg_relative=0, motion_kind=0, pitch_amp_deg=0.0, pitch_freq=0.0,
-                 pivot_x=0.0, pivot_y=0.0, tile_cfg=-1, cg_precond=0, tc_tile=0):
+                 pivot_x=0.0, pivot_y=0.0, tile_cfg=-1, cg_precond=0, tc_tile=0, refine_slices=0):
     return Options(precision, cg_relative, motion_kind, pitch_amp_deg, pitch_freq, pivot_x, pivot_y,
-                   tile_cfg, cg_precond, tc_tile)
+                   tile_cfg, cg_precond, tc_tile, refine_slices)
 
 
 class Solver:

@@ -76,6 +76,11 @@ typedef struct {
                           128 (K blocks of 64) or 256 (K blocks of 32); 0 = the measured
                           autotuner picks per launch group. Taken from the first case of
                           a batch                                                  */
+  int refine_slices;   /* split-precision form: BF16 slices per operand in the refinement
+                          sweep's correction solve: 3 (six products; 0 selects it) or 2
+                          (three products, about ten times the error, half that
+                          pass's tensor-core work). Taken from the first case of a
+                          batch                                                    */
 } ibfs_options_c;
 
 typedef struct ibfs_handle ibfs_handle;

@@ -12,7 +12,7 @@ Cases:
   * a 5-level cylinder on 128x128 cells, 30 steps, both forms;
   * one batch holding one case of every grid size of the batched workload
     (128, 192, 256, 384, 512) and every level count 2..5, both forms;
-  * the split form over 400 steps of a 128x128x3 plate.
+  * the split form over 400 steps of a 128x128x3 plate (CFL 0.2).
 
 Bars: the plain FP64 method within 1e-10, the split-precision form within
 1e-8, on
@@ -44,7 +44,9 @@ SPLIT_TOL = 1e-8
 CYL200 = W.cylinder_re100()
 PLATE400 = W.plate_re300()
 CYL128_L5 = W.case(128, 5, 100.0, 0.004, "cylinder")
-PLATE128_LONG = W.case(128, 3, 300.0, 0.4 * 4.0 / 128, "plate", aoa=30.0)
+# CFL 0.2: at the batched workload's CFL 0.4 this case diverges after ~130
+# steps in the oracle as on the GPU (the explicit Adams-Bashforth term's limit)
+PLATE128_LONG = W.case(128, 3, 300.0, 0.2 * 4.0 / 128, "plate", aoa=30.0)
 # one case of each grid size of the batched workload and each level count 2..5
 MIX = [W.case(128, 5, 80.0, 0.4 * 4.0 / 128, "cylinder"),
        W.case(192, 2, 300.0, 0.4 * 4.0 / 192, "plate", aoa=20.0),

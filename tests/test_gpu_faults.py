@@ -55,7 +55,7 @@ def test_singular_force_system_is_chol_error():
 
 @pytest.mark.parametrize("entry", ["advance", "advance_n"])
 def test_tensor_core_wait_limit_gives_timeout(entry):
-    m, lev = 64, 3
+    m, lev = 256, 3
     xb, yb = W.circle(4.0 / m)
     p = C.make_params(m, m, 0.004, 100.0, lev)
     g = C.Solver(p, (xb, yb), C.make_options(precision=1))
