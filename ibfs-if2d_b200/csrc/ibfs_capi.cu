@@ -210,7 +210,7 @@ static int num_sms() {
   return sms;
 }
 
-static int tune_gemm(const std::vector<GemmDesc>& ds, bool dual, cudaStream_t st) {
+static int tune_gemm(const std::vector<GemmDesc>& ds, bool dual, cudaStream_t st, bool allow_split = true) {
   // A group with few 32x32 tiles (one or a few cases) leaves SMs idle: it gets
   // a split-K cluster configuration, chosen by the tile count alone and never
   // by timing, so that a group shape gets the same configuration -- the same
@@ -219,7 +219,7 @@ static int tune_gemm(const std::vector<GemmDesc>& ds, bool dual, cudaStream_t st
   // bit-identical results, so timing noise never changes a result.
   long tiles32 = 0;
   for (auto& d : ds) tiles32 += gemm_tiles(d.M, d.N, 1);
-  if (tiles32 < 2L * num_sms()) return tiles32 >= num_sms() / 2 ? 4 : 6;
+  if (allow_split && tiles32 < 2L * num_sms()) return tiles32 >= num_sms() / 2 ? 4 : 6;
   const int fallback = [&] {
     long tiles64 = 0;
     for (auto& d : ds) tiles64 += gemm_tiles(d.M, d.N, 0);
@@ -279,10 +279,12 @@ int tuned_gemm_sites() {
 struct ProgBuilder {
   ibfs_handle* h;
   Prog& P;
+  bool allow_split = true;  // split-K tiles for groups with few tiles (not for preprocess, see factor_cases)
   void add(std::function<void()> fn, int tag = TAG_STENCIL, double flops = 0.0) { P.push_back({fn, tag, flops}); }
   void gemm(std::vector<GemmDesc> ds, bool dual) {
     if (ds.empty()) return;
-    const int cfg = h->tile_cfg >= 0 && h->tile_cfg < kGemmF64Cfgs ? h->tile_cfg : tune_gemm(ds, dual, h->st);
+    const int cfg =
+        h->tile_cfg >= 0 && h->tile_cfg < kGemmF64Cfgs ? h->tile_cfg : tune_gemm(ds, dual, h->st, allow_split);
     int mt = 0;
     for (auto& d : ds) mt = std::max(mt, gemm_tiles(d.M, d.N, cfg));
     GemmDesc* dd = dupload(h, ds);
@@ -711,7 +713,12 @@ static int factor_cases(ibfs_handle* h, const std::vector<int>& need) {
     ibfs_handle tmp;  // collects this chunk's uploads
     tmp.tile_cfg = h->tile_cfg;
     tmp.st = h->st;
+    // the columns are packed into chunks by memory budget, so a case's GEMM
+    // groups here depend on what it is batched with: only the unsplit tile
+    // shapes (bit-identical to each other) keep its factor the same alone
+    // and in any batch
     ProgBuilder B{&tmp, P};
+    B.allow_split = false;
     DevCase* dsh = dupload(&tmp, sh);
     const int* dids = B.ints(ids);
     const int* dcols = B.ints(cols);
@@ -1099,7 +1106,7 @@ static int finish_create(ibfs_handle* h) {
     });
     if (rc) return fail(rc, precision_error());
     precision_set_tile(h->prec, h->cases[0].o.tc_tile);
-    precision_set_refine_slices(h->prec, h->cases[0].o.refine_slices);
+    precision_set_refine(h->prec, h->cases[0].o.refine_slices, h->cases[0].o.poisson_sweeps);
   }
   build_step_program(h);
   IBFS_CUDA_CHECK(cudaDeviceSynchronize());
@@ -1164,8 +1171,9 @@ static int check_device_waits(ibfs_handle* h) {
   IBFS_CUDA_CHECK(cudaStreamSynchronize(h->st));
   if (!(st4[0] & 2)) return IBFS_OK;
   static const char* roles[] = {"?", "producer waiting for a free stage", "MMA waiting for a free accumulator",
-                                "MMA waiting for a loaded stage", "epilogue waiting for an accumulator"};
-  const int r = (st4[1] >= 1 && st4[1] <= 4) ? st4[1] : 0;
+                                "MMA waiting for a loaded stage", "epilogue waiting for an accumulator",
+                                "probe wait of the timeout test"};
+  const int r = (st4[1] >= 1 && st4[1] <= 5) ? st4[1] : 0;
   std::string msg = std::string("a bounded device wait gave up (tensor-core GEMM: ") + roles[r] + ", block " +
                     std::to_string(st4[2]) + ", step " + std::to_string(st4[3]) + ")";
   if (st4[0] & 4) msg += "; a drain of in-flight copies also gave up";
@@ -1512,11 +1520,11 @@ int ibfs_profile_step(ibfs_handle* h, double* ms, int* launches, double* flops) 
   return wrc;
 }
 
-int ibfs_set_wait_limit(ibfs_handle* h, double seconds) {
+int ibfs_set_wait_limit(ibfs_handle* h, double seconds, int probe) {
   if (!h || !(seconds >= 0.0) || seconds > 60.0)
     return fail(IBFS_ERR_ARG, "ibfs_set_wait_limit: seconds must be in [0, 60]");
   if (!h->prec) return IBFS_OK;  // plain FP64 handles have no bounded device waits
-  int rc = precision_set_wait_limit(h->prec, seconds);
+  int rc = precision_set_wait_limit(h->prec, seconds, probe);
   if (rc) return fail(rc, "ibfs_set_wait_limit: cannot write the limit to the device");
   return IBFS_OK;
 }

@@ -115,7 +115,8 @@ __device__ __forceinline__ bool mbar_spin(uint32_t bar, uint32_t parity, uint64_
 // A wait that gave up: flag the error (bit 2 of status[0]) and, for the first
 // one, record where: status[1] = role (1 producer/stage free, 2 MMA/accumulator
 // free, 3 MMA/stage loaded, 4 epilogue/accumulator ready), status[2] = block,
-// status[3] = pipeline step. A drain wait that gave up sets bit 4.
+// status[3] = pipeline step; role 5 is the probe of the timeout test. A drain
+// wait that gave up sets bit 4.
 __device__ __forceinline__ void report_timeout(int* status, int role, int step) {
   atomicOr(status, 2);
   if (atomicCAS(status + 1, 0, role) == 0) {
@@ -394,17 +395,18 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   float* stg_all = reinterpret_cast<float*>(smem + S * SB);
-  uint64_t* bars = (uint64_t*)(smem + S * SB + kPEpi);  // full[2] empty[2] accf[2] acce[2]
-  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + kPEpi + 8 * 8);
+  uint64_t* bars = (uint64_t*)(smem + S * SB + kPEpi);  // full[2] empty[2] accf[2] acce[2] probe
+  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + kPEpi + 9 * 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t sbase = smem_u32(smem);
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]);
   const uint32_t accf0 = smem_u32(&bars[4]), acce0 = smem_u32(&bars[6]);
-  const uint64_t lim = *wait_ns;
+  const uint64_t lim = wait_ns[0];
   if (warp == 0) tmem_alloc(smem_u32(tmem_slot), TCOLS);
   if (tid == 0) {
     for (int b = 0; b < 6; b++) mbar_init(smem_u32(&bars[b]), 1);
     for (int b = 6; b < 8; b++) mbar_init(smem_u32(&bars[b]), kPEpiWarps);
+    mbar_init(smem_u32(&bars[8]), 1);  // probe: nothing ever arrives on it
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
@@ -412,6 +414,16 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
   const uint32_t tmem = *tmem_slot;
   const int G = gridDim.x;
   bool to = false;
+  // Test of the timeout path (wait_ns[1] != 0): before any copy or product is
+  // issued, every role waits on the probe barrier, which nothing completes,
+  // so each wait gives up after the limit and the block returns through the
+  // same exit as a real timeout, with nothing in flight.
+  if (wait_ns[1] != 0 && (tid == 0 || tid == 32 || warp >= 2)) {
+    if (!mbar_wait(smem_u32(&bars[8]), 0, lim)) {
+      report_timeout(status, 5, 0);
+      to = true;
+    }
+  }
 
   if (tid == 0) {  // TMA producer
     int g = 0;
@@ -490,7 +502,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     const int c0 = ((warp - 2) >> 2) * CH;        // the warp's half of the tile's columns
     float* stg = stg_all + (warp - 2) * (32 * 33);
     int t = 0;
-    for (int w = blockIdx.x; w < nwork; w += G, t++) {
+    for (int w = blockIdx.x; w < nwork && !to; w += G, t++) {
       const int a = t & 1, u = t >> 1;
       if (!mbar_wait(accf0 + 8 * a, u & 1, lim)) { report_timeout(status, 4, t); to = true; break; }
       tc_fence_after();
@@ -631,9 +643,10 @@ struct PrecisionPlan {
   std::map<int, std::pair<bf16*, long long>> sine;  // N+1 -> slices
   std::map<int, float*> lam;                        // N+1 -> 1-D eigenvalues
   int* status = nullptr;
-  unsigned long long* wait_ns = nullptr;  // limit of the GEMM's waits, ns (device word)
+  unsigned long long* wait_ns = nullptr;  // device words: limit of the GEMM's waits (ns), probe flag
   int tc_tile = 0;                        // output tile width: 0 = the measured autotuner, 128 or 256
-  int refine_slices = 3;                  // slices per operand of the correction solve (3 or 2)
+  int refine_slices = 0;                  // slices per operand of the correction solves: 0 = by kind, 2 or 3
+  int poisson_sweeps = 2;                 // correction sweeps of the Poisson (ctci) solves: 1 or 2
   std::vector<int> tile_choice;           // width used by each GEMM launch group, in build order
   Alloc alloc;
 };
@@ -726,12 +739,12 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
   }
   pp->status = cases.empty() ? (int*)alloc(sizeof(int) * 4) : cases[0].status;
-  pp->wait_ns = (unsigned long long*)alloc(sizeof(unsigned long long));
+  pp->wait_ns = (unsigned long long*)alloc(2 * sizeof(unsigned long long));
   if (!pp->wait_ns) {
     g_perr = "device allocation failed for the wait limit";
     return 8;
   }
-  if (precision_set_wait_limit(pp, (double)kWaitLimitNs * 1e-9)) {
+  if (precision_set_wait_limit(pp, (double)kWaitLimitNs * 1e-9, 0)) {
     g_perr = "cannot set the wait limit";
     return 4;
   }
@@ -781,14 +794,17 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
 void precision_free(PrecisionPlan* pp) { delete pp; }
 
 void precision_set_tile(PrecisionPlan* pp, int width) { pp->tc_tile = (width == 128 || width == 256) ? width : 0; }
-void precision_set_refine_slices(PrecisionPlan* pp, int slices) { pp->refine_slices = slices == 2 ? 2 : 3; }
+void precision_set_refine(PrecisionPlan* pp, int slices, int poisson_sweeps) {
+  pp->refine_slices = (slices == 2 || slices == 3) ? slices : 0;
+  pp->poisson_sweeps = poisson_sweeps == 1 ? 1 : 2;
+}
 const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp) { return pp->tile_choice; }
 void precision_reset_tile_choices(PrecisionPlan* pp) { pp->tile_choice.clear(); }
 
-int precision_set_wait_limit(PrecisionPlan* pp, double seconds) {
+int precision_set_wait_limit(PrecisionPlan* pp, double seconds, int probe) {
   if (!pp || !pp->wait_ns || !(seconds >= 0.0) || seconds > 60.0) return 7;
-  const unsigned long long ns = (unsigned long long)(seconds * 1e9);
-  return cudaMemcpy(pp->wait_ns, &ns, sizeof(ns), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : 4;
+  const unsigned long long w[2] = {(unsigned long long)(seconds * 1e9), probe ? 1ull : 0ull};
+  return cudaMemcpy(pp->wait_ns, w, sizeof(w), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : 4;
 }
 const char* precision_error() { return g_perr.c_str(); }
 
@@ -945,9 +961,24 @@ static void add_prep(PrecisionPlan* pp, Prog& P, const std::vector<PrepDesc>& ds
 }
 
 // The eight GEMMs + two assembly passes of a batch of refined solves.
+// Refinement of a batch of solves of one kind. Each correction pass forms the
+// residual r = v - A x in FP64 with the exact 5-point stencil and adds S f S r.
+// Why the Poisson solves (ctci, A = C^T C) get a second correction sweep: the
+// FP32 accumulation leaves white noise of relative size e ~ 3e-7 in x; A
+// lifts its high modes (lambda up to 8) into r, and the noise of the next
+// transform of r, spread back over all modes, is lifted by 1/lambda_min at the
+// low modes, so each sweep contracts the error only by kappa*e, kappa =
+// lambda_max/lambda_min ~ 0.4 m^2 (~0.03 at m = 512). The Crank-Nicolson and
+// ainv operators, A = I + nu C^T C, have kappa = 1 + 8 nu (~1-5): one sweep
+// with two slices per operand (three products) leaves ~1e-11 there.
 static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, cudaStream_t st) {
   if (rq.empty()) return;
-  for (int pass = 0; pass < 2; pass++) {
+  const bool poisson = rq[0].fkind == F_LAMINV;
+  const int npass = 1 + (poisson ? pp->poisson_sweeps : 1);
+  // slice products of a correction pass: three slices (six products) for the
+  // Poisson solves, two (three products) for the others, unless fixed
+  const int np_corr = pp->refine_slices == 3 ? 6 : pp->refine_slices == 2 ? 3 : (poisson ? 6 : 3);
+  for (int pass = 0; pass < npass; pass++) {
     std::vector<PrepDesc> prep;
     std::vector<TcDesc> g1, g2, g3, g4;
     for (auto& r : rq) {
@@ -957,7 +988,7 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       pd.m = c.m; pd.n = c.n;
       pd.Xs = b.Xs; pd.sX = b.sX; pd.ld = b.ldX;
       pd.out64 = nullptr;
-      if (pass == 1) {
+      if (pass >= 1) {
         pd.x0 = r.out;
         pd.res = r.fkind == F_LAMINV ? RES_LAP : RES_AOP;
         pd.nu = 0.5 * c.dt / (c.delta * c.delta * std::pow(4.0, r.k - 1) * c.re);
@@ -982,11 +1013,7 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       TcDesc L2 = L1;  // x = S_m * T'
       L2.epi = pass == 0 ? TC_F64_STORE : TC_F64_ADD;
       L2.C64 = r.out; L2.ldc = M;
-      // the correction solve acts on a residual already ~1e-6 of the data;
-      // with three slices per operand (six products) its own error is set by
-      // the FP32 accumulation (~1e-6), with two (three products) by the
-      // slices' 16 significant bits (~1e-5), ten times larger in the result
-      int np = pass == 0 ? 6 : (pp->refine_slices == 2 ? 3 : 6);
+      const int np = pass == 0 ? 6 : np_corr;
       R.nprod = np;
       L1.nprod = np;
       L2.nprod = np;

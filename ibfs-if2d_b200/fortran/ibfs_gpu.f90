@@ -38,6 +38,7 @@ MODULE ibfs_gpu
      INTEGER(C_INT) :: cg_precond
      INTEGER(C_INT) :: tc_tile
      INTEGER(C_INT) :: refine_slices
+     INTEGER(C_INT) :: poisson_sweeps
   END TYPE ibfs_options_c
 
   INTERFACE
@@ -122,6 +123,14 @@ MODULE ibfs_gpu
        INTEGER(C_INT), INTENT(IN) :: npt(*)
        REAL(C_DOUBLE), INTENT(IN) :: u_j(*), u_j_osc(*), omg_j(*), theta_j(*)
      END FUNCTION ibfs_set_actuators
+
+     ! limit (seconds) of the split-precision GEMM's bounded device waits
+     INTEGER(C_INT) FUNCTION ibfs_set_wait_limit(h, seconds, probe) BIND(C, name="ibfs_set_wait_limit")
+       IMPORT :: C_INT, C_DOUBLE, C_PTR
+       TYPE(C_PTR), VALUE :: h
+       REAL(C_DOUBLE), VALUE :: seconds
+       INTEGER(C_INT), VALUE :: probe
+     END FUNCTION ibfs_set_wait_limit
 
      TYPE(C_PTR) FUNCTION ibfs_last_error(h) BIND(C, name="ibfs_last_error")
        IMPORT :: C_PTR

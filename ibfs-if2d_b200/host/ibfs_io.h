@@ -29,7 +29,7 @@ bool parse_read_parameters(const std::string& text, ibfs_params_c& p, std::strin
 
 // Optional &B200_OPTIONS group of the same file (precision, cg_relative,
 // motion_kind, pitch_amp_deg, pitch_freq, pivot_x, pivot_y, tile_cfg,
-// cg_precond, tc_tile, refine_slices); a
+// cg_precond, tc_tile, refine_slices, poisson_sweeps); a
 // Fortran READ of &READ_PARAMETERS skips it. Returns false on a malformed
 // group; absent group = zero-initialised options (reference behaviour).
 bool parse_b200_options(const std::string& text, ibfs_options_c& o, std::string& msg);

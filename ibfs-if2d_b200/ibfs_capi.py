@@ -49,6 +49,7 @@ class Options(ctypes.Structure):
         ("pitch_amp_deg", ctypes.c_double), ("pitch_freq", ctypes.c_double),
         ("pivot_x", ctypes.c_double), ("pivot_y", ctypes.c_double), ("tile_cfg", ctypes.c_int),
         ("cg_precond", ctypes.c_int), ("tc_tile", ctypes.c_int), ("refine_slices", ctypes.c_int),
+        ("poisson_sweeps", ctypes.c_int),
     ]
 
 
@@ -97,7 +98,7 @@ def lib():
         L.ibfs_adjoint_pitch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]
         L.ibfs_set_actuators.argtypes = [vp, ctypes.c_int, ctypes.c_int, _IP, _DP, _DP, _DP, _DP]
         L.ibfs_profile_step.argtypes = [vp, _DP, _IP, _DP]
-        L.ibfs_set_wait_limit.argtypes = [vp, ctypes.c_double]
+        L.ibfs_set_wait_limit.argtypes = [vp, ctypes.c_double, ctypes.c_int]
         L.ibfs_gemm_tiles.argtypes = [vp, _IP, ctypes.c_int]
         L.ibfs_dst2d_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
@@ -121,9 +122,10 @@ def make_params(m, n, dt, re, mgridlev, len_=4.0, offsetx=2.0, offsety=2.0, stat
 
 
 def make_options(precision=0, cg_relative=0, motion_kind=0, pitch_amp_deg=0.0, pitch_freq=0.0,
-                 pivot_x=0.0, pivot_y=0.0, tile_cfg=-1, cg_precond=0, tc_tile=0, refine_slices=0):
+                 pivot_x=0.0, pivot_y=0.0, tile_cfg=-1, cg_precond=0, tc_tile=0, refine_slices=0,
+                 poisson_sweeps=0):
     return Options(precision, cg_relative, motion_kind, pitch_amp_deg, pitch_freq, pivot_x, pivot_y,
-                   tile_cfg, cg_precond, tc_tile, refine_slices)
+                   tile_cfg, cg_precond, tc_tile, refine_slices, poisson_sweeps)
 
 
 class Solver:
@@ -304,9 +306,10 @@ class Solver:
             return float(J[0]), float(dJ[0]), ms_f.value, ms_t.value
         return J, dJ, ms_f.value, ms_t.value
 
-    def set_wait_limit(self, seconds):
-        """Limit of the bounded device waits (ibfs_set_wait_limit)."""
-        self._check(lib().ibfs_set_wait_limit(self.h, float(seconds)))
+    def set_wait_limit(self, seconds, probe=False):
+        """Limit of the bounded device waits; probe=True makes every GEMM block
+        wait first on a barrier nothing completes (ibfs_set_wait_limit)."""
+        self._check(lib().ibfs_set_wait_limit(self.h, float(seconds), int(bool(probe))))
 
     def last_cg_iterations(self):
         return lib().ibfs_last_cg_iterations(self.h)

@@ -76,11 +76,16 @@ typedef struct {
                           128 (K blocks of 64) or 256 (K blocks of 32); 0 = the measured
                           autotuner picks per launch group. Taken from the first case of
                           a batch                                                  */
-  int refine_slices;   /* split-precision form: BF16 slices per operand in the refinement
-                          sweep's correction solve: 3 (six products; 0 selects it) or 2
-                          (three products, about ten times the error, half that
-                          pass's tensor-core work). Taken from the first case of a
-                          batch                                                    */
+  int refine_slices;   /* split-precision form: BF16 slices per operand in the correction
+                          solves of the refinement: 0 = three (six products) for the
+                          Poisson solves of vort2flux, two (three products) for the
+                          well-conditioned Crank-Nicolson and ainv solves; 2 or 3 = that
+                          many for all. Taken from the first case of a batch       */
+  int poisson_sweeps;  /* split-precision form: FP64 residual-correction sweeps of the
+                          Poisson (ctci) solves: 0 or 2 = two, 1 = one (each sweep
+                          contracts their error by ~0.4 m^2 x 3e-7, ~0.03 at m = 512;
+                          the other solves always get one). Taken from the first
+                          case of a batch                                          */
 } ibfs_options_c;
 
 typedef struct ibfs_handle ibfs_handle;
@@ -276,12 +281,14 @@ int ibfs_dst2d_noalloc(const double* d_in, double* d_out, int m, int n, void* st
  * work, wait for its own copies and products still in flight, free its
  * tensor memory and return; the advance then returns IBFS_ERR_TIMEOUT with
  * the role, block and pipeline step of the first wait that gave up, and the
- * handle's state is undefined (destroy it). A limit of 0 makes every wait
- * that does not succeed at once give up, which exercises this path. The
- * value is read by the kernel from device memory, so it applies to captured
- * step graphs too. No reference counterpart (the reference has no device
+ * handle's state is undefined (destroy it). probe != 0 tests that path: every
+ * thread block of the GEMM first waits on a barrier that nothing completes,
+ * before it issues any copy or product, so each such wait gives up after
+ * `seconds` and the next advance returns IBFS_ERR_TIMEOUT. The values are
+ * read by the kernel from device memory, so they apply to captured step
+ * graphs too. No reference counterpart (the reference has no device
  * waits). */
-int ibfs_set_wait_limit(ibfs_handle* h, double seconds);
+int ibfs_set_wait_limit(ibfs_handle* h, double seconds, int probe);
 
 /* Message of the last error on this handle (or of the last failed create). */
 const char* ibfs_last_error(const ibfs_handle* h);

@@ -8,8 +8,8 @@
 * Pitching plate on the moving-body grid (chord 1 about mid-chord, Re 500,
   512x512 cells, 5 levels, dt 0.001, CG to a relative 1e-12, preconditioned),
   started at the phase of maximum pitch: derivative of the mean drag over the
-  last 3 of 6 steps with respect to the pitch amplitude against a fourth-order
-  central difference.
+  last 3 of 6 steps with respect to the pitch amplitude against fourth-order
+  central differences.
 """
 import numpy as np
 import pytest
@@ -98,8 +98,16 @@ def test_pitch_adjoint_on_the_moving_body_grid():
     J, g, ms_f, ms_t = s.adjoint_pitch_run(PSTEPS, 3, wx, np.zeros(PSTEPS))
     s.close()
     assert abs(J - _pitch_J(amp)) <= 1e-12 * abs(J)
-    h = 0.02
-    Jp1, Jm1, Jp2, Jm2 = (_pitch_J(amp + d) for d in (h, -h, 2 * h, -2 * h))
-    fd = (8.0 * (Jp1 - Jm1) - (Jp2 - Jm2)) / (12.0 * h)
-    print(f"pitching plate 512x512x5: dJ/dA adjoint {g:.10e}, fourth-order FD {fd:.10e}")
-    assert abs(g - fd) <= 1e-6 * abs(fd), (g, fd)
+    # The body points' regularisation weights are C1 in the point positions
+    # (Roma-Peskin-Berger kernel, grid.f90:233-249), so J(A) bends sharply
+    # wherever a point's support crosses a face; on this grid (dx = 0.0078) a
+    # 0.02 degree step moves the points by ~0.02 dx and the fourth-order
+    # difference is off by ~6e-4. Steps of 0.002 and 0.001 degrees (J is
+    # repeatable to 1e-15 at CG's relative 1e-12) resolve the derivative.
+    fds = {}
+    for h in (0.002, 0.001):
+        Jp1, Jm1, Jp2, Jm2 = (_pitch_J(amp + d) for d in (h, -h, 2 * h, -2 * h))
+        fds[h] = (8.0 * (Jp1 - Jm1) - (Jp2 - Jm2)) / (12.0 * h)
+    print(f"pitching plate 512x512x5: dJ/dA adjoint {g:.10e}, fourth-order FD {fds}")
+    for h, fd in fds.items():
+        assert abs(g - fd) <= 1e-6 * abs(fd), (h, g, fd)

@@ -6,11 +6,12 @@ traps or hangs the GPU:
   point outside the grid has no faces within the support of its delta kernel,
   so its row and column of A are zero and choldc meets a zero pivot; the oracle
   fails on the same input;
-* the bounded waits of the tensor-core GEMM, given a limit of zero through
-  ibfs_set_wait_limit, give up: the advance returns IBFS_ERR_TIMEOUT naming the
-  wait, each thread block first waits for its own copies and products in
-  flight and frees its tensor memory, and a new handle then advances normally
-  (its GEMM allocates the same tensor memory on every SM);
+* a bounded wait of the tensor-core GEMM runs out: ibfs_set_wait_limit's probe
+  makes every thread block wait on a barrier that nothing completes (2 ms
+  limit) before it issues any copy or product; the advance returns
+  IBFS_ERR_TIMEOUT naming that wait, each block frees its tensor memory, and a
+  new handle then advances normally (its GEMM allocates the same tensor memory
+  on every SM);
 * the host driver stops with IBFS_ERR_IO on a truncated restart record or
   Cholesky record in a real (non dry-run) run.
 """
@@ -55,20 +56,20 @@ def test_singular_force_system_is_chol_error():
 
 @pytest.mark.parametrize("entry", ["advance", "advance_n"])
 def test_tensor_core_wait_limit_gives_timeout(entry):
-    m, lev = 256, 3
+    m, lev = 128, 3
     xb, yb = W.circle(4.0 / m)
     p = C.make_params(m, m, 0.004, 100.0, lev)
     g = C.Solver(p, (xb, yb), C.make_options(precision=1))
-    g.precompute()  # the factor is FP64 (no tensor-core GEMM); made before the limit drops
-    g.set_wait_limit(0.0)
+    g.precompute()  # the factor is FP64 (no tensor-core GEMM); made before the probe is set
+    g.set_wait_limit(0.002, probe=True)  # every GEMM block waits on a barrier nothing completes
     with pytest.raises(C.IbfsError) as e:
         if entry == "advance":
             g.advance()
         else:
             g.advance_n(2, want_hist=False)
     assert e.value.code == C.ERR_TIMEOUT, str(e.value)
-    assert "bounded device wait gave up" in str(e.value)
-    assert "drain" not in str(e.value)  # every in-flight copy and product completed before exit
+    assert "bounded device wait gave up" in str(e.value) and "probe" in str(e.value)
+    assert "drain" not in str(e.value)  # nothing was in flight when the blocks returned
     g.close()
     # a fresh handle: its GEMM allocates tensor memory on every SM again and
     # its results follow the oracle at the split-precision bar
@@ -80,8 +81,8 @@ def test_tensor_core_wait_limit_gives_timeout(entry):
         assert rc == 0
     assert abs(og["fx"][0] - o["fx"][0]) / abs(o["fx"][0]) < 1e-8
     assert rel(g2.get_state()["omega"], oc.get_state()["omega"]) < 1e-8
-    # the default limit back on an existing handle: still runs
-    g2.set_wait_limit(1.0)
+    # a short real limit on a healthy handle does not fire; a bad one is refused
+    g2.set_wait_limit(0.5)
     g2.advance_n(2, want_hist=False)
     with pytest.raises(C.IbfsError) as e:
         g2.set_wait_limit(-1.0)
