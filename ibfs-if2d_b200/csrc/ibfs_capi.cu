@@ -1433,11 +1433,11 @@ int ibfs_output_stride(const ibfs_handle* h) { return h ? h->out_stride : 0; }
 
 int ibfs_kernels_per_step(const ibfs_handle* h) { return h ? h->graph_kernels : -1; }
 
-int ibfs_gemm_tiles(const ibfs_handle* h, int* widths, int max) {
+int ibfs_gemm_tiles(const ibfs_handle* h, int* cfgs, int max) {
   if (!h) return -1;
   if (!h->prec) return 0;
   const std::vector<int>& w = precision_tile_choices(h->prec);
-  for (int i = 0; widths && i < (int)w.size() && i < max; i++) widths[i] = w[i];
+  for (int i = 0; cfgs && i < (int)w.size() && i < max; i++) cfgs[i] = w[i];
   return (int)w.size();
 }
 

@@ -20,13 +20,15 @@ void precision_free(PrecisionPlan* pp);
 // Limit (seconds, 0..60) of every bounded wait of the tensor-core GEMM;
 // probe != 0 makes every block wait first on a barrier nothing completes.
 int precision_set_wait_limit(PrecisionPlan* pp, double seconds, int probe);
-// Output tile width of the tensor-core GEMM: 128, 256, or 0 for the autotuner.
-void precision_set_tile(PrecisionPlan* pp, int width);
+// Tile configuration of the tensor-core GEMM: 1 (128x128, K blocks of 64, two
+// stages), 2 (128x256, K 32, two stages), 3 (128x128, K 32, four stages), or 0
+// for the measured autotuner.
+void precision_set_tile(PrecisionPlan* pp, int cfg);
 // Refinement: slices per operand of the correction solves (0 = three for the
 // Poisson solves, two for the others; 2 or 3 = all) and correction sweeps of
 // the Poisson (ctci) solves (1 or 2).
 void precision_set_refine(PrecisionPlan* pp, int slices, int poisson_sweeps);
-// Widths chosen for the GEMM launch groups built since the last reset.
+// Configurations chosen for the GEMM launch groups built since the last reset.
 const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp);
 void precision_reset_tile_choices(PrecisionPlan* pp);
 const char* precision_error();

@@ -202,14 +202,15 @@ enum TcFactor { F_NONE = 0, F_LAMINV = 1, F_LAM1I_NORM = 2 };
 
 // One GEMM of one (case, level) item. Operands are 3-slice BF16 arrays
 // [slice][row][k] (k contiguous) described by TMA tensor maps; A rows are
-// output rows, B rows output columns. mapA/mapB serve the 128 x 128 output
-// tile (box 64 k x 128 rows, 128-byte swizzle), mapA2/mapB2 the 128 x 256
-// tile (box 32 k x 128 / 256 rows, 64-byte swizzle).
+// output rows, B rows output columns. K blocks of 64 (128-byte swizzle): mapA
+// and mapB (boxes of 128 rows); K blocks of 32 (64-byte swizzle): mapA2 (128
+// rows), mapB2 (256 rows) and mapB3 (128 rows).
 struct __align__(64) TcDesc {
   CUtensorMap mapA;
   CUtensorMap mapB;
   CUtensorMap mapA2;
   CUtensorMap mapB2;
+  CUtensorMap mapB3;
   int M, N, Kp;   // logical output extents; K padded to a multiple of 64
   int tiles_m;    // 128-row output tiles
   int nprod;      // slice products: 6 (three slices per operand) or 3 (two slices: A0B0 + A0B1 + A1B0)
@@ -269,20 +270,26 @@ struct TcWork {
   int desc, tile;
 };
 
-// Output tile 128 x BN: BN = 128 with K blocks of 64 (128-byte rows), or
-// BN = 256 with K blocks of 32 (64-byte rows); two pipeline stages each.
-template <int BN> struct TcShape;
-template <> struct TcShape<128> { static constexpr int BK = 64; };
-template <> struct TcShape<256> { static constexpr int BK = 32; };
-template <int BN> constexpr int tc_ab() { return 128 * TcShape<BN>::BK * 2; }   // one A slice tile
-template <int BN> constexpr int tc_bb() { return BN * TcShape<BN>::BK * 2; }    // one B slice tile
-template <int BN> constexpr int tc_stage() { return 3 * tc_ab<BN>() + 3 * tc_bb<BN>(); }  // 96 KB / 72 KB
+// Tile configurations of the tensor-core GEMM (output tile 128 x BN, K blocks
+// of BK, S pipeline stages of the three A and three B slice tiles), kTcCfgs of
+// them:
+//   1: BN 128, BK 64, 2 stages of 96 KB (128-byte rows, 128-byte swizzle)
+//   2: BN 256, BK 32, 2 stages of 72 KB (64-byte rows, 64-byte swizzle)
+//   3: BN 128, BK 32, 4 stages of 48 KB: the same tile as 1 with twice the
+//      loads in flight ahead of the MMAs (three stages, ~2.3k cycles of MMA
+//      at six products, against one stage of ~1.5k cycles in 1)
+constexpr int kTcCfgs = 3;
+template <int BN, int BK> constexpr int tc_ab() { return 128 * BK * 2; }  // one A slice tile
+template <int BN, int BK> constexpr int tc_bb() { return BN * BK * 2; }   // one B slice tile
+template <int BN, int BK> constexpr int tc_stage() { return 3 * tc_ab<BN, BK>() + 3 * tc_bb<BN, BK>(); }
 constexpr int kPEpiWarps = 8;                                  // two warps per TMEM lane quarter
 constexpr int kPThreads = 64 + 32 * kPEpiWarps;
 constexpr int kPEpi = kPEpiWarps * 32 * 33 * 4;                // per-warp 32 x 33 FP32 staging
-template <int BN> constexpr int tc_smem() { return 2 * tc_stage<BN>() + kPEpi + 1024 + 256; }
-static_assert(tc_smem<128>() <= 232448, "persistent GEMM shared memory above the per-CTA limit");
-static_assert(tc_smem<256>() <= 232448, "persistent GEMM shared memory above the per-CTA limit");
+constexpr int kPBars = 256;                                    // barriers and the TMEM address slot
+template <int BN, int BK, int S> constexpr int tc_smem() { return S * tc_stage<BN, BK>() + kPEpi + 1024 + kPBars; }
+static_assert(tc_smem<128, 64, 2>() <= 232448, "persistent GEMM shared memory above the per-CTA limit");
+static_assert(tc_smem<256, 32, 2>() <= 232448, "persistent GEMM shared memory above the per-CTA limit");
+static_assert(tc_smem<128, 32, 4>() <= 232448, "persistent GEMM shared memory above the per-CTA limit");
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
@@ -385,28 +392,31 @@ __device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t tr
   }
 }
 
-template <int BN>
+template <int BN, int BK, int S>
 __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* __restrict__ descs,
                                                             const TcWork* __restrict__ work, int nwork,
                                                             int* __restrict__ status,
                                                             const unsigned long long* __restrict__ wait_ns) {
-  constexpr int BK = TcShape<BN>::BK, S = 2, AB = tc_ab<BN>(), BB = tc_bb<BN>(), SB = tc_stage<BN>();
+  constexpr int AB = tc_ab<BN, BK>(), BB = tc_bb<BN, BK>(), SB = tc_stage<BN, BK>();
   constexpr uint32_t TCOLS = 2 * BN;  // double-buffered FP32 accumulator columns
+  static_assert((2 * S + 5) * 8 + 4 <= kPBars, "barrier area");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   float* stg_all = reinterpret_cast<float*>(smem + S * SB);
-  uint64_t* bars = (uint64_t*)(smem + S * SB + kPEpi);  // full[2] empty[2] accf[2] acce[2] probe
-  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + kPEpi + 9 * 8);
+  // full[S] empty[S] accf[2] acce[2] probe, then the TMEM address
+  uint64_t* bars = (uint64_t*)(smem + S * SB + kPEpi);
+  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + kPEpi + (2 * S + 5) * 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t sbase = smem_u32(smem);
-  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]);
-  const uint32_t accf0 = smem_u32(&bars[4]), acce0 = smem_u32(&bars[6]);
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[S]);
+  const uint32_t accf0 = smem_u32(&bars[2 * S]), acce0 = smem_u32(&bars[2 * S + 2]);
+  const uint32_t probe = smem_u32(&bars[2 * S + 4]);
   const uint64_t lim = wait_ns[0];
   if (warp == 0) tmem_alloc(smem_u32(tmem_slot), TCOLS);
   if (tid == 0) {
-    for (int b = 0; b < 6; b++) mbar_init(smem_u32(&bars[b]), 1);
-    for (int b = 6; b < 8; b++) mbar_init(smem_u32(&bars[b]), kPEpiWarps);
-    mbar_init(smem_u32(&bars[8]), 1);  // probe: nothing ever arrives on it
+    for (int b = 0; b < 2 * S + 2; b++) mbar_init(smem_u32(&bars[b]), 1);
+    for (int b = 2 * S + 2; b < 2 * S + 4; b++) mbar_init(smem_u32(&bars[b]), kPEpiWarps);
+    mbar_init(probe, 1);  // probe: nothing ever arrives on it
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
@@ -419,7 +429,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
   // so each wait gives up after the limit and the block returns through the
   // same exit as a real timeout, with nothing in flight.
   if (wait_ns[1] != 0 && (tid == 0 || tid == 32 || warp >= 2)) {
-    if (!mbar_wait(smem_u32(&bars[8]), 0, lim)) {
+    if (!mbar_wait(probe, 0, lim)) {
       report_timeout(status, 5, 0);
       to = true;
     }
@@ -433,11 +443,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       const int m0 = (tile % d.tiles_m) * 128, n0 = (tile / d.tiles_m) * BN;
       const int nk = d.Kp / BK;
       const int ns = d.nprod == 3 ? 2 : 3;  // slices per operand
-      const CUtensorMap* mA = BN == 128 ? &d.mapA : &d.mapA2;
-      const CUtensorMap* mB = BN == 128 ? &d.mapB : &d.mapB2;
+      const CUtensorMap* mA = BK == 64 ? &d.mapA : &d.mapA2;
+      const CUtensorMap* mB = BK == 64 ? &d.mapB : (BN == 256 ? &d.mapB2 : &d.mapB3);
       for (int kb = 0; kb < nk; kb++, g++) {
-        const int s = g & 1;
-        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g >> 1) + 1) & 1, lim)) { report_timeout(status, 1, g); to = true; break; }
+        const int s = g % S;
+        // stage s is free once the MMAs of load g - S completed (its empty phase (g - S) / S)
+        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g / S) + 1) & 1, lim)) { report_timeout(status, 1, g); to = true; break; }
         const uint32_t fb = full0 + 8 * s;
         mbar_expect_tx(fb, ns * (AB + BB));
         const uint32_t st = sbase + s * SB;
@@ -450,7 +461,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
     // its load). Their full-barrier phases complete when their bytes land;
     // in a run without timeouts they have completed already.
     for (int gi = g - 1; gi >= 0 && gi >= g - S; gi--)
-      if (!mbar_spin(full0 + 8 * (gi & 1), (gi >> 1) & 1, kDrainLimitNs)) atomicOr(status, 4);
+      if (!mbar_spin(full0 + 8 * (gi % S), (gi / S) & 1, kDrainLimitNs)) atomicOr(status, 4);
   } else if (tid == 32) {  // MMA issuer
     constexpr int pa[6] = {0, 0, 1, 0, 1, 2};
     constexpr int pb[6] = {0, 1, 0, 2, 1, 0};
@@ -468,8 +479,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
       const int np = d.nprod == 3 ? 3 : 6;
       const uint32_t acc = tmem + a * BN;
       for (int kb = 0; kb < nk; kb++, g++) {
-        const int s = g & 1;
-        if (!mbar_spin(full0 + 8 * s, (g >> 1) & 1, lim)) { report_timeout(status, 3, g); to = true; break; }
+        const int s = g % S;
+        if (!mbar_spin(full0 + 8 * s, (g / S) & 1, lim)) { report_timeout(status, 3, g); to = true; break; }
         tc_fence_after();
         // stage base descriptor; operand tiles and K steps are immediate
         // offsets (16-byte units) on its address field
@@ -485,7 +496,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
         }
         umma_commit(empty0 + 8 * s);
         last_bar = empty0 + 8 * s;
-        last_par = (g >> 1) & 1;
+        last_par = (g / S) & 1;
       }
       if (!to) {
         umma_commit(accf0 + 8 * a);
@@ -569,9 +580,14 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
   const int i0 = (bm.y % ti) * 32, j0 = (bm.y / ti) * 32;
   __shared__ double t[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  for (int jj = ty; jj < 32; jj += 8) {
-    int i = i0 + tx, j = j0 + jj;
+  // the thread's four nodes are assembled in registers before any store, so
+  // their loads are in flight together
+  double vv[4], v64[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int i = i0 + tx, j = j0 + ty + 8 * e;
     double v = 0.0;
+    v64[e] = 0.0;
     if (i < M && j < N) {
       size_t o = i + (size_t)j * M;
       v = d.src_scale * d.src[o];
@@ -582,13 +598,19 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
           v = apply_bc_at(v, a, b, d.m, d.n, 1.0,
                           [&](int side, int I) { return getbc_raw(d.bcsrc, d.m, d.n, side, I) * 1.0; });
       }
-      if (d.out64) d.out64[o] = v;
+      v64[e] = v;
       if (d.x0) {
         double ax = d.res == RES_LAP ? lap5(d.x0, i, j, M, N) : d.x0[o] + d.nu * lap5(d.x0, i, j, M, N);
         v = v - ax;
       }
     }
-    t[jj][tx] = v;
+    vv[e] = v;
+  }
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int i = i0 + tx, j = j0 + ty + 8 * e;
+    if (d.out64 && i < M && j < N) d.out64[i + (size_t)j * M] = v64[e];
+    t[ty + 8 * e][tx] = vv[e];
   }
   __syncthreads();
   const int ii = threadIdx.x >> 3, g = threadIdx.x & 7;  // row ii, columns 4g .. 4g+3
@@ -634,6 +656,7 @@ struct CaseBufs {
   int ldSm, ldSn;
   CUtensorMap mapX, mapT, mapSm, mapSn;      // K blocks of 64: A roles 128 rows, B roles 128 rows
   CUtensorMap mapX2, mapT2, mapSm2, mapSn2;  // K blocks of 32: A roles 128 rows, B roles 256 rows
+  CUtensorMap mapT3, mapSn3;                 // K blocks of 32: B roles 128 rows
   const float* lamx;
   const float* lamy;
 };
@@ -644,10 +667,10 @@ struct PrecisionPlan {
   std::map<int, float*> lam;                        // N+1 -> 1-D eigenvalues
   int* status = nullptr;
   unsigned long long* wait_ns = nullptr;  // device words: limit of the GEMM's waits (ns), probe flag
-  int tc_tile = 0;                        // output tile width: 0 = the measured autotuner, 128 or 256
+  int tc_tile = 0;                        // tile configuration: 0 = the measured autotuner, 1..3
   int refine_slices = 0;                  // slices per operand of the correction solves: 0 = by kind, 2 or 3
   int poisson_sweeps = 2;                 // correction sweeps of the Poisson (ctci) solves: 1 or 2
-  std::vector<int> tile_choice;           // width used by each GEMM launch group, in build order
+  std::vector<int> tile_choice;           // configuration of each GEMM launch group, in build order
   Alloc alloc;
 };
 
@@ -726,10 +749,12 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   pp->alloc = alloc;
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_gemm_tc_persist<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_gemm_tc_persist<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<256>()) !=
-            cudaSuccess) {
+    if (cudaFuncSetAttribute(k_gemm_tc_persist<128, 64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc_smem<128, 64, 2>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc_persist<256, 32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc_smem<256, 32, 2>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc_persist<128, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc_smem<128, 32, 4>()) != cudaSuccess) {
       g_perr = "cannot raise shared memory limit for the tensor-core GEMM";
       return 4;
     }
@@ -782,7 +807,8 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
         !make_map(&b.mapSm, b.Sm, Km, Rs_m, b.sSm, 64, 128) || !make_map(&b.mapSn, b.Sn, Kn, Rs_n, b.sSn, 64, 128) ||
         !make_map(&b.mapX2, b.Xs, Kn, Rm, b.sX, 32, 128) || !make_map(&b.mapT2, b.Ts, Km, Rn, b.sT, 32, 256) ||
         !make_map(&b.mapSm2, b.Sm, Km, Rs_m, b.sSm, 32, 128) ||
-        !make_map(&b.mapSn2, b.Sn, Kn, Rs_n, b.sSn, 32, 256)) {
+        !make_map(&b.mapSn2, b.Sn, Kn, Rs_n, b.sSn, 32, 256) || !make_map(&b.mapT3, b.Ts, Km, Rn, b.sT, 32, 128) ||
+        !make_map(&b.mapSn3, b.Sn, Kn, Rs_n, b.sSn, 32, 128)) {
       g_perr = "cuTensorMapEncodeTiled failed";
       return 4;
     }
@@ -793,7 +819,7 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
 
 void precision_free(PrecisionPlan* pp) { delete pp; }
 
-void precision_set_tile(PrecisionPlan* pp, int width) { pp->tc_tile = (width == 128 || width == 256) ? width : 0; }
+void precision_set_tile(PrecisionPlan* pp, int cfg) { pp->tc_tile = (cfg >= 1 && cfg <= kTcCfgs) ? cfg : 0; }
 void precision_set_refine(PrecisionPlan* pp, int slices, int poisson_sweeps) {
   pp->refine_slices = (slices == 2 || slices == 3) ? slices : 0;
   pp->poisson_sweeps = poisson_sweeps == 1 ? 1 : 2;
@@ -826,10 +852,14 @@ static T* upload(PrecisionPlan* pp, const std::vector<T>& v) {
   return p;
 }
 
-// Work list of one launch group for output tiles 128 x bn: every tile of
+// Output tile width of a tile configuration (1..3, see TcShape above).
+static inline int tc_bn(int cfg) { return cfg == 2 ? 256 : 128; }
+
+// Work list of one launch group for tile configuration cfg: every tile of
 // every descriptor, sorted by K length (longest first) for balance across the
 // SMs.
-static std::vector<TcWork> tc_work(const std::vector<TcDesc>& ds, int bn) {
+static std::vector<TcWork> tc_work(const std::vector<TcDesc>& ds, int cfg) {
+  const int bn = tc_bn(cfg);
   std::vector<TcWork> wl;
   for (int i = 0; i < (int)ds.size(); i++) {
     const int tiles = ds[i].tiles_m * ((ds[i].N + bn - 1) / bn);
@@ -839,23 +869,24 @@ static std::vector<TcWork> tc_work(const std::vector<TcDesc>& ds, int bn) {
   return wl;
 }
 
-static void launch_tc(int bn, const TcDesc* dd, const TcWork* dw, int nw, int* status, const unsigned long long* wait_ns,
-                      cudaStream_t st) {
+static void launch_tc(int cfg, const TcDesc* dd, const TcWork* dw, int nw, int* status,
+                      const unsigned long long* wait_ns, cudaStream_t st) {
   const int grid = std::min(nw, g_num_sms > 0 ? g_num_sms : 148);
-  if (bn == 256)
-    k_gemm_tc_persist<256><<<grid, kPThreads, tc_smem<256>(), st>>>(dd, dw, nw, status, wait_ns);
+  if (cfg == 2)
+    k_gemm_tc_persist<256, 32, 2><<<grid, kPThreads, tc_smem<256, 32, 2>(), st>>>(dd, dw, nw, status, wait_ns);
+  else if (cfg == 3)
+    k_gemm_tc_persist<128, 32, 4><<<grid, kPThreads, tc_smem<128, 32, 4>(), st>>>(dd, dw, nw, status, wait_ns);
   else
-    k_gemm_tc_persist<128><<<grid, kPThreads, tc_smem<128>(), st>>>(dd, dw, nw, status, wait_ns);
+    k_gemm_tc_persist<128, 64, 2><<<grid, kPThreads, tc_smem<128, 64, 2>(), st>>>(dd, dw, nw, status, wait_ns);
 }
 
-// Measured autotuner of the tensor-core GEMM's output tile (128 x 128 with K
-// blocks of 64, or 128 x 256 with K blocks of 32). A launch group is timed
-// once with each shape -- its outputs redirected to a scratch buffer, its
-// operands read where they lie, so no state changes -- and the faster shape
-// is kept, cached per process and device by the group's shape signature.
-// Both shapes issue the same slice products; only the order of the FP32
-// accumulation differs (K blocks of 32 against 64), which the refinement
-// sweep's FP64 residual absorbs.
+// Measured autotuner of the tensor-core GEMM's tile configuration. A launch
+// group is timed once with each configuration -- its outputs redirected to a
+// scratch buffer, its operands read where they lie, so no state changes --
+// and the fastest is kept, cached per process and device by the group's shape
+// signature. All configurations issue the same slice products; only the order
+// of the FP32 accumulation differs (K blocks of 32 against 64), which the
+// refinement's FP64 residual absorbs.
 static std::mutex g_tc_mu;
 static std::map<std::string, int> g_tc_tuned;
 
@@ -882,14 +913,14 @@ static int tune_tc(PrecisionPlan* pp, const std::vector<TcDesc>& ds, cudaStream_
     if (d.epi == TC_SPLIT_COL || d.epi == TC_SCALE_SPLIT_ROW) need = std::max(need, (size_t)(3 * d.sC) * sizeof(bf16));
     else need = std::max(need, (size_t)d.ldc * d.N * sizeof(double));
   }
-  int best = 128;
+  int best = 1;
   void* scratch = nullptr;
   TcDesc* dd = nullptr;
   TcWork* dw = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   std::vector<TcDesc> t = ds;
   size_t maxw = 0;
-  for (int bn : {128, 256}) maxw = std::max(maxw, tc_work(ds, bn).size());
+  for (int cfg = 1; cfg <= kTcCfgs; cfg++) maxw = std::max(maxw, tc_work(ds, cfg).size());
   if (cudaMalloc(&scratch, need) == cudaSuccess && cudaMalloc(&dd, sizeof(TcDesc) * t.size()) == cudaSuccess &&
       cudaMalloc(&dw, sizeof(TcWork) * maxw) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
       cudaEventCreate(&e1) == cudaSuccess) {
@@ -900,19 +931,19 @@ static int tune_tc(PrecisionPlan* pp, const std::vector<TcDesc>& ds, cudaStream_
     }
     cudaMemcpy(dd, t.data(), sizeof(TcDesc) * t.size(), cudaMemcpyHostToDevice);
     float best_ms = 1e30f;
-    for (int bn : {128, 256}) {
-      const std::vector<TcWork> wl = tc_work(ds, bn);
+    for (int cfg = 1; cfg <= kTcCfgs; cfg++) {
+      const std::vector<TcWork> wl = tc_work(ds, cfg);
       cudaMemcpy(dw, wl.data(), sizeof(TcWork) * wl.size(), cudaMemcpyHostToDevice);
       const int nw = (int)wl.size();
-      launch_tc(bn, dd, dw, nw, pp->status, pp->wait_ns, st);  // warm-up
+      launch_tc(cfg, dd, dw, nw, pp->status, pp->wait_ns, st);  // warm-up
       cudaEventRecord(e0, st);
-      for (int r = 0; r < 3; r++) launch_tc(bn, dd, dw, nw, pp->status, pp->wait_ns, st);
+      for (int r = 0; r < 3; r++) launch_tc(cfg, dd, dw, nw, pp->status, pp->wait_ns, st);
       cudaEventRecord(e1, st);
       float ms = 0.f;
       if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
           ms < best_ms) {
         best_ms = ms;
-        best = bn;
+        best = cfg;
       }
     }
   }
@@ -926,13 +957,13 @@ static int tune_tc(PrecisionPlan* pp, const std::vector<TcDesc>& ds, cudaStream_
   return best;
 }
 
-// One persistent launch over every tile of every descriptor, with the output
-// tile the handle's option or the autotuner chose.
+// One persistent launch over every tile of every descriptor, with the tile
+// configuration the handle's option or the autotuner chose.
 static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& ds, cudaStream_t st) {
   if (ds.empty()) return;
-  const int bn = pp->tc_tile == 128 || pp->tc_tile == 256 ? pp->tc_tile : tune_tc(pp, ds, st);
-  pp->tile_choice.push_back(bn);
-  std::vector<TcWork> wl = tc_work(ds, bn);
+  const int cfg = pp->tc_tile >= 1 && pp->tc_tile <= kTcCfgs ? pp->tc_tile : tune_tc(pp, ds, st);
+  pp->tile_choice.push_back(cfg);
+  std::vector<TcWork> wl = tc_work(ds, cfg);
   double fl = 0.0;
   for (auto& d : ds) fl += 2.0 * d.M * (double)d.N * (double)(d.epi == TC_SPLIT_COL ? d.N : d.M);
   TcDesc* dd = upload(pp, ds);
@@ -940,7 +971,7 @@ static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDes
   const int nw = (int)wl.size();
   int* status = pp->status;
   const unsigned long long* wait_ns = pp->wait_ns;
-  P.push_back({[=]() { launch_tc(bn, dd, dw, nw, status, wait_ns, st); }, TAG_GEMM_TC, fl});
+  P.push_back({[=]() { launch_tc(cfg, dd, dw, nw, status, wait_ns, st); }, TAG_GEMM_TC, fl});
 }
 
 static void add_gemm(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& all, cudaStream_t st) {
@@ -1000,12 +1031,12 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       int tm = (M + 127) / 128;
       TcDesc R{};  // T = X * S_n
       R.mapA = b.mapX; R.mapB = b.mapSn;
-      R.mapA2 = b.mapX2; R.mapB2 = b.mapSn2;
+      R.mapA2 = b.mapX2; R.mapB2 = b.mapSn2; R.mapB3 = b.mapSn3;
       R.M = M; R.N = N; R.Kp = rup(N, 64); R.tiles_m = tm;
       R.epi = TC_SPLIT_COL; R.Cs = b.Ts; R.sC = b.sT; R.ldcs = b.ldT;
       TcDesc L1{};  // U = f .* (S_m * T)
       L1.mapA = b.mapSm; L1.mapB = b.mapT;
-      L1.mapA2 = b.mapSm2; L1.mapB2 = b.mapT2;
+      L1.mapA2 = b.mapSm2; L1.mapB2 = b.mapT2; L1.mapB3 = b.mapT3;
       L1.M = M; L1.N = N; L1.Kp = rup(M, 64); L1.tiles_m = tm;
       L1.epi = TC_SCALE_SPLIT_ROW; L1.fkind = r.fkind; L1.Cs = b.Xs; L1.sC = b.sX; L1.ldcs = b.ldX;
       L1.lamx = b.lamx; L1.lamy = b.lamy; L1.norm = (float)c.norm;

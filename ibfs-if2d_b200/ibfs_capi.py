@@ -318,7 +318,7 @@ class Solver:
         return lib().ibfs_kernels_per_step(self.h)
 
     def gemm_tiles(self):
-        """Output tile widths of the tensor-core GEMM launch groups of the step."""
+        """Tile configurations (1..3) of the tensor-core GEMM launch groups of the step."""
         n = lib().ibfs_gemm_tiles(self.h, None, 0)
         out = np.zeros(max(n, 1), dtype=np.int32)
         lib().ibfs_gemm_tiles(self.h, out.ctypes.data_as(_IP), n)

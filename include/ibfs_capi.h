@@ -72,10 +72,11 @@ typedef struct {
                           applied as z = Q L_k^-T L_k^-1 Q^T r with Q the remaining
                           rotation of each point's (fx, fy); a body that does not move
                           has one slot. Same stop rule on the true residual        */
-  int tc_tile;         /* split-precision form: output tile width of the tensor-core GEMM,
-                          128 (K blocks of 64) or 256 (K blocks of 32); 0 = the measured
-                          autotuner picks per launch group. Taken from the first case of
-                          a batch                                                  */
+  int tc_tile;         /* split-precision form: tile configuration of the tensor-core
+                          GEMM: 1 = 128x128 output tile, K blocks of 64, two pipeline
+                          stages; 2 = 128x256, K blocks of 32, two stages; 3 = 128x128,
+                          K blocks of 32, four stages; 0 = the measured autotuner picks
+                          per launch group. Taken from the first case of a batch   */
   int refine_slices;   /* split-precision form: BF16 slices per operand in the correction
                           solves of the refinement: 0 = three (six products) for the
                           Poisson solves of vort2flux, two (three products) for the
@@ -185,11 +186,12 @@ int ibfs_last_timing(const ibfs_handle* h, double* ms);
  * counterpart; reports the launch structure of the advance). */
 int ibfs_kernels_per_step(const ibfs_handle* h);
 
-/* Output tile widths (128 or 256) of the split-precision form's tensor-core
- * GEMM launch groups of the step program, in launch order: writes up to max
- * of them to widths (may be NULL) and returns how many there are (0 for a
- * plain FP64 handle). No reference counterpart (reports the tuner's choice). */
-int ibfs_gemm_tiles(const ibfs_handle* h, int* widths, int max);
+/* Tile configurations (1..3, as ibfs_options_c.tc_tile) of the
+ * split-precision form's tensor-core GEMM launch groups of the step program,
+ * in launch order: writes up to max of them to cfgs (may be NULL) and
+ * returns how many there are (0 for a plain FP64 handle). No reference
+ * counterpart (reports the tuner's choice). */
+int ibfs_gemm_tiles(const ibfs_handle* h, int* cfgs, int max);
 
 /* Discrete adjoint of nsteps advances (no reference counterpart; the
  * reference has no derivatives). For a single-case handle, stationary body,
