@@ -343,11 +343,23 @@ def split_error_long_horizon(C, plate_steps=5000, batch_steps=1000):
         state[prec] = g.get_state()
         L = g.sizes[0]["nlev"]
         g.close()
+    # the flow's own sensitivity: the plain FP64 advance again with another
+    # summation order of its transforms (unsplit 32x32 tiles against the
+    # split-K tiles the tuner gives a single case), a perturbation of ~1e-16
+    g = C.Solver(params[0], bodies[0], C.make_options(precision=0, tile_cfg=1))
+    h_alt = g.advance_n(plate_steps)
+    g.close()
+    fr = _force_errors(h_alt, hist[0], (0, 1))
     fe = _force_errors(hist[1], hist[0], (0, 1))
+    marks = [s for s in (1, 10, 100, 1000, 2000, 3000, 4000, 5000) if s <= plate_steps]
+    out["plate400_fp64_summation_order"] = {
+        "steps": plate_steps, "force_err_max": float(fr.max()),
+        "force_err_at": {str(s): float(fr[s - 1]) for s in marks},
+        "basis": "plain FP64 with unsplit 32x32 transform tiles vs plain FP64 with the split-K tiles: the "
+                 "growth of a round-off perturbation over the horizon"}
     out["plate400"] = {"workload": PLATE["workload"], "steps": plate_steps, "force_err_max": float(fe.max()),
                        "force_err_argmax_step": int(fe.argmax()) + 1,
-                       "force_err_at": {str(s): float(fe[s - 1]) for s in (1, 100, 1000, 2000, 3000, 4000, 5000)
-                                        if s <= plate_steps},
+                       "force_err_at": {str(s): float(fe[s - 1]) for s in marks},
                        **_level_errors(state[1], state[0], L)}
     cases = W.batch(BATCH["ncases"], seed=SEED)
     ids, _ = W.stratified_sample(cases)
