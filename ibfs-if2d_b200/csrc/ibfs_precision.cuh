@@ -26,7 +26,7 @@ int precision_set_wait_limit(PrecisionPlan* pp, double seconds, int probe);
 void precision_set_tile(PrecisionPlan* pp, int cfg);
 // Refinement: slices per operand of the correction solves (0 = three for the
 // Poisson solves, two for the others; 2 or 3 = all) and correction sweeps of
-// the Poisson (ctci) solves (1 or 2).
+// the Poisson (ctci) solves (1, the default, or 2).
 void precision_set_refine(PrecisionPlan* pp, int slices, int poisson_sweeps);
 // Configurations chosen for the GEMM launch groups built since the last reset.
 const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp);

@@ -580,14 +580,9 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
   const int i0 = (bm.y % ti) * 32, j0 = (bm.y / ti) * 32;
   __shared__ double t[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  // the thread's four nodes are assembled in registers before any store, so
-  // their loads are in flight together
-  double vv[4], v64[4];
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const int i = i0 + tx, j = j0 + ty + 8 * e;
+  for (int jj = ty; jj < 32; jj += 8) {
+    int i = i0 + tx, j = j0 + jj;
     double v = 0.0;
-    v64[e] = 0.0;
     if (i < M && j < N) {
       size_t o = i + (size_t)j * M;
       v = d.src_scale * d.src[o];
@@ -598,19 +593,13 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
           v = apply_bc_at(v, a, b, d.m, d.n, 1.0,
                           [&](int side, int I) { return getbc_raw(d.bcsrc, d.m, d.n, side, I) * 1.0; });
       }
-      v64[e] = v;
+      if (d.out64) d.out64[o] = v;
       if (d.x0) {
         double ax = d.res == RES_LAP ? lap5(d.x0, i, j, M, N) : d.x0[o] + d.nu * lap5(d.x0, i, j, M, N);
         v = v - ax;
       }
     }
-    vv[e] = v;
-  }
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const int i = i0 + tx, j = j0 + ty + 8 * e;
-    if (d.out64 && i < M && j < N) d.out64[i + (size_t)j * M] = v64[e];
-    t[ty + 8 * e][tx] = vv[e];
+    t[jj][tx] = v;
   }
   __syncthreads();
   const int ii = threadIdx.x >> 3, g = threadIdx.x & 7;  // row ii, columns 4g .. 4g+3
@@ -669,7 +658,7 @@ struct PrecisionPlan {
   unsigned long long* wait_ns = nullptr;  // device words: limit of the GEMM's waits (ns), probe flag
   int tc_tile = 0;                        // tile configuration: 0 = the measured autotuner, 1..3
   int refine_slices = 0;                  // slices per operand of the correction solves: 0 = by kind, 2 or 3
-  int poisson_sweeps = 2;                 // correction sweeps of the Poisson (ctci) solves: 1 or 2
+  int poisson_sweeps = 1;                 // correction sweeps of the Poisson (ctci) solves: 1 or 2
   std::vector<int> tile_choice;           // configuration of each GEMM launch group, in build order
   Alloc alloc;
 };
@@ -822,7 +811,7 @@ void precision_free(PrecisionPlan* pp) { delete pp; }
 void precision_set_tile(PrecisionPlan* pp, int cfg) { pp->tc_tile = (cfg >= 1 && cfg <= kTcCfgs) ? cfg : 0; }
 void precision_set_refine(PrecisionPlan* pp, int slices, int poisson_sweeps) {
   pp->refine_slices = (slices == 2 || slices == 3) ? slices : 0;
-  pp->poisson_sweeps = poisson_sweeps == 1 ? 1 : 2;
+  pp->poisson_sweeps = poisson_sweeps == 2 ? 2 : 1;
 }
 const std::vector<int>& precision_tile_choices(const PrecisionPlan* pp) { return pp->tile_choice; }
 void precision_reset_tile_choices(PrecisionPlan* pp) { pp->tile_choice.clear(); }
@@ -994,7 +983,8 @@ static void add_prep(PrecisionPlan* pp, Prog& P, const std::vector<PrepDesc>& ds
 // The eight GEMMs + two assembly passes of a batch of refined solves.
 // Refinement of a batch of solves of one kind. Each correction pass forms the
 // residual r = v - A x in FP64 with the exact 5-point stencil and adds S f S r.
-// Why the Poisson solves (ctci, A = C^T C) get a second correction sweep: the
+// Why the Poisson solves (ctci, A = C^T C) may need a second correction sweep
+// (poisson_sweeps = 2; one is the default): the
 // FP32 accumulation leaves white noise of relative size e ~ 3e-7 in x; A
 // lifts its high modes (lambda up to 8) into r, and the noise of the next
 // transform of r, spread back over all modes, is lifted by 1/lambda_min at the

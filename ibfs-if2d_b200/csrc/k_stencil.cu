@@ -62,11 +62,9 @@ __device__ __forceinline__ double uavg_c(const double* __restrict__ q, double u0
 }
 
 // The per-node values of the level update's right-hand side: returns rhsA =
-// con1*rhs + con2*rhs_old + rhsbc and sets rhs (the new rhs_old,
-// operators.f90:112-133); loads only, so that callers can batch several nodes
-// before their stores.
+// con1*rhs + con2*rhs_old + rhsbc and stores rhs_old = rhs (operators.f90:112-133).
 template <bool Q0C>
-__device__ __forceinline__ double rhs_value(const DevCase& C, LevelItem it, int t, int first_step, double& rhs_out) {
+__device__ __forceinline__ double rhs_value(const DevCase& C, LevelItem it, int t, int first_step) {
   int m = C.m, n = C.n;
   int i = t % (m - 1) + 2, j = t / (m - 1) + 2;
   int k = it.k;
@@ -117,7 +115,7 @@ __device__ __forceinline__ double rhs_value(const DevCase& C, LevelItem it, int 
   double del22 = C.delta * C.delta * (double)(1 << (2 * (k - 1)));
   double con1 = 1.5 * C.dt / del22 / C.norm;
   double con2 = -0.5 * C.dt / del22 / C.norm;
-  rhs_out = rhs;
+  ro[t] = rhs;
   return con1 * rhs + con2 * rold + rb;
 }
 
@@ -130,25 +128,10 @@ __global__ void __launch_bounds__(256) k_rhs(const DevCase* __restrict__ cases, 
   const LevelItem it = items[bm.x];
   const DevCase& C = cases[it.c];
   const int tend = min(C.ns, bm.y + kBlockElems);
-  double* ro = C.rhs_old + (size_t)(it.k - 1) * C.ns;
-  // the block's four nodes per thread are computed before any of them is
-  // stored, so their loads are in flight together
-  constexpr int E = kBlockElems / 256;
-  double ra[E], rh[E];
-  const bool q0c = C.q0_const != 0;
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const int t = bm.y + (int)threadIdx.x + 256 * e;
-    ra[e] = rh[e] = 0.0;
-    if (t < tend) ra[e] = q0c ? rhs_value<true>(C, it, t, first_step, rh[e]) : rhs_value<false>(C, it, t, first_step, rh[e]);
-  }
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const int t = bm.y + (int)threadIdx.x + 256 * e;
-    if (t < tend) {
-      C.rhsA[t] = ra[e];
-      ro[t] = rh[e];
-    }
+  if (C.q0_const) {
+    for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) C.rhsA[t] = rhs_value<true>(C, it, t, first_step);
+  } else {
+    for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) C.rhsA[t] = rhs_value<false>(C, it, t, first_step);
   }
 }
 
@@ -196,31 +179,17 @@ __global__ void __launch_bounds__(256) k_rhs_split(const DevCase* __restrict__ c
   __shared__ double tile[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   const bool q0c = C.q0_const != 0;
-  double* ro = C.rhs_old + (size_t)(it.k - 1) * C.ns;
-  // four nodes per thread, all computed before any store (their loads overlap)
-  double vv[4], rh[4];
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const int i = i0 + tx, j = j0 + ty + 8 * e;
-    vv[e] = 0.0;
-    rh[e] = 0.0;
+  for (int jj = ty; jj < 32; jj += 8) {
+    const int i = i0 + tx, j = j0 + jj;
+    double v = 0.0;
     if (i < M && j < N) {
       const int t = i + j * M;
-      const double rA = q0c ? rhs_value<true>(C, it, t, first_step, rh[e])
-                            : rhs_value<false>(C, it, t, first_step, rh[e]);
-      double v = d.scale * rA;
-      vv[e] = v + (om[t] - d.nu * lap5_nodes(om, i, j, M, N));
+      const double rA = q0c ? rhs_value<true>(C, it, t, first_step) : rhs_value<false>(C, it, t, first_step);
+      v = d.scale * rA;
+      v = v + (om[t] - d.nu * lap5_nodes(om, i, j, M, N));
+      d.b64[t] = v;
     }
-  }
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const int i = i0 + tx, j = j0 + ty + 8 * e;
-    if (i < M && j < N) {
-      const int t = i + j * M;
-      ro[t] = rh[e];
-      d.b64[t] = vv[e];
-    }
-    tile[ty + 8 * e][tx] = vv[e];
+    tile[jj][tx] = v;
   }
   __syncthreads();
   const int ii = threadIdx.x >> 3, g = threadIdx.x & 7;  // row ii, columns 4g .. 4g+3

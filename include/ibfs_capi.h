@@ -83,7 +83,7 @@ typedef struct {
                           well-conditioned Crank-Nicolson and ainv solves; 2 or 3 = that
                           many for all. Taken from the first case of a batch       */
   int poisson_sweeps;  /* split-precision form: FP64 residual-correction sweeps of the
-                          Poisson (ctci) solves: 0 or 2 = two, 1 = one (each sweep
+                          Poisson (ctci) solves: 0 or 1 = one, 2 = two (each sweep
                           contracts their error by ~0.4 m^2 x 3e-7, ~0.03 at m = 512;
                           the other solves always get one). Taken from the first
                           case of a batch                                          */
