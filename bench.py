@@ -190,16 +190,18 @@ def algorithmic_transform_flops(cases, nlev):
     return tot
 
 
-def issued_tensor_flops(cases, nlev, refine_products=6):
-    """Slice products actually issued per step by the split form: every solve
-    is 4 GEMMs of 6 products (first pass) + 4 of refine_products (correction),
-    on 128-row and 128-column padded tiles with K padded to 64; 3L+1 solves
-    per case."""
+def issued_tensor_flops(cases, nlev):
+    """Slice products actually issued per step by the split form (default
+    refinement): every solve is 4 GEMMs of 6 products (first pass) plus 4 of
+    the correction's products -- 6 for the 2L Poisson solves of the two
+    vort2flux calls, 3 for the L Crank-Nicolson solves and ainv -- on
+    128-row and 128-column padded tiles with K padded to 64."""
     rup = lambda x, a: (x + a - 1) // a * a
     tot = 0.0
     for c, L in zip(cases, nlev):
         N = c["m"] - 1
-        tot += (3 * L + 1) * 4 * 2.0 * rup(N, 128) ** 2 * rup(N, 64) * (6 + refine_products)
+        per_product = 4 * 2.0 * rup(N, 128) ** 2 * rup(N, 64)
+        tot += per_product * (2 * L * (6 + 6) + (L + 1) * (6 + 3))
     return tot
 
 
