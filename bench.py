@@ -282,8 +282,12 @@ def plain_and_split_plate(C, torch, steps, warmup, flush):
         for s in range(warmup + steps):
             flush.zero_()
             torch.cuda.synchronize()
+            if s >= warmup:  # lets a profiler select the timed steps of each form
+                torch.cuda.nvtx.range_push(f"plate_timed_{'fp64' if prec == 0 else 'split'}")
             g.advance_n(1, want_hist=False)
             if s >= warmup:
+                torch.cuda.synchronize()
+                torch.cuda.nvtx.range_pop()
                 times.append(g.last_ms())
         ms = sum(times) / len(times)
         out[prec] = {"value": cells / (ms / 1e3), "ms_per_step": ms, "cells_per_step": cells,
