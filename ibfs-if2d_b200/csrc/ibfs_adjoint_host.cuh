@@ -8,7 +8,9 @@
 //      (omega, rhs_old, q, fb, itime) every K steps and the forces of every step;
 //   2. backward pass, segment by segment from the last: restore the segment's
 //      checkpoint, recompute its K steps storing each step-start state, then
-//      run the adjoint step backwards through the segment.
+//      run the adjoint step backwards through the segment. The forward pass
+//      stores the last segment's step-start states itself, so that segment is
+//      not recomputed.
 // The adjoint step is one fixed launch program (captured as a CUDA graph);
 // per step only the pointers to the stored forward state and the objective
 // weights change, uploaded into the device AdjCase array before each replay.
@@ -319,12 +321,16 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
   cudaEvent_t e0, e1, e2;
   cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
   cudaEventRecord(e0, h->st);
-  // 1. forward pass with checkpoints
+  // 1. forward pass with checkpoints; the last segment's step-start states go
+  // straight into the segment buffer, so the backward pass starts without
+  // recomputing it
+  const int s_last = (nck - 1) * K;
   for (int s = 0; s < nsteps && rc == IBFS_OK; s++) {
     if (s % K == 0) {
       adj_save(h, P, ck + P.state * (s / K));
       cudaMemcpyAsync(ck_it + s / K, c.itime, sizeof(int), cudaMemcpyDeviceToDevice, h->st);
     }
+    if (s >= s_last) adj_save(h, P, seg + P.state * (s - s_last));
     rc = run_step(h);
     cudaMemcpyAsync(hist + (size_t)s * h->out_stride, h->d_out, sizeof(double) * h->out_stride,
                     cudaMemcpyDeviceToDevice, h->st);
@@ -351,10 +357,12 @@ static int adj_run(ibfs_handle* h, int nsteps, int K, const double* body_vel, co
   for (int sg = nck - 1; sg >= 0 && rc == IBFS_OK; sg--) {
     int s0 = sg * K, s1 = std::min(nsteps, s0 + K);
     cudaStreamSynchronize(h->st);  // the pinned slots of the previous segment are free
-    // recompute the segment's step-start states; the first is the checkpoint
+    // recompute the segment's step-start states (the last segment's are
+    // already there from the forward pass); the first is the checkpoint
     // itself and the last step's result is not needed
-    cudaMemcpyAsync(seg, ck + P.state * sg, sizeof(double) * P.state, cudaMemcpyDeviceToDevice, h->st);
-    if (s1 - s0 > 1) {
+    if (sg != nck - 1)
+      cudaMemcpyAsync(seg, ck + P.state * sg, sizeof(double) * P.state, cudaMemcpyDeviceToDevice, h->st);
+    if (sg != nck - 1 && s1 - s0 > 1) {
       adj_restore(h, P, ck + P.state * sg);
       cudaMemcpyAsync(c.itime, ck_it + sg, sizeof(int), cudaMemcpyDeviceToDevice, h->st);
       for (int s = s0; s < s1 - 1 && rc == IBFS_OK; s++) {
