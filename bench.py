@@ -725,9 +725,8 @@ def run_ours(args):
             "roofline": roof, "roofline_step_hbm": roof_step, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": kern * args.steps, "kernels_per_step": kern, "profile_step": prof,
             "gemm_tiles": {name: g.gemm_tiles().count(cfg) for cfg, name in
-                           ((1, "128x128/K64/2 stages"), (2, "128x256/K32/2 stages"), (3, "128x128/K32/4 stages"))},
-            "gemm_tiles": {name: g.gemm_tiles().count(cfg) for cfg, name in
-                           ((1, "128x128/K64/2 stages"), (2, "128x256/K32/2 stages"), (3, "128x128/K32/4 stages"))},
+                           ((1, "128x128/K64/2 stages"), (2, "128x256/K32/2 stages"), (3, "128x128/K32/4 stages"),
+                            (4, "256x256 CTA pair/K64/2 stages"))},
             "clocks": cs.summary(), "impl": "ours",
         }
         out.update(extras)

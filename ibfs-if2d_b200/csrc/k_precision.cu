@@ -278,7 +278,9 @@ struct TcWork {
 //   3: BN 128, BK 32, 4 stages of 48 KB: the same tile as 1 with twice the
 //      loads in flight ahead of the MMAs (three stages, ~2.3k cycles of MMA
 //      at six products, against one stage of ~1.5k cycles in 1)
-constexpr int kTcCfgs = 3;
+//   4: a 256 x 256 tile on a pair of CTAs (k_gemm_tc_pair), BK 64, 2 stages
+//      of 96 KB per CTA
+constexpr int kTcCfgs = 4;
 template <int BN, int BK> constexpr int tc_ab() { return 128 * BK * 2; }  // one A slice tile
 template <int BN, int BK> constexpr int tc_bb() { return BN * BK * 2; }   // one B slice tile
 template <int BN, int BK> constexpr int tc_stage() { return 3 * tc_ab<BN, BK>() + 3 * tc_bb<BN, BK>(); }
@@ -535,6 +537,219 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc_persist(const TcDesc* 
 }
 
 // ---------------------------------------------------------------------------
+// CTA-pair form (tile configuration 4): a cluster of two CTAs on two SMs
+// computes one 256 x 256 output tile with tcgen05.mma.cta_group::2 (M 256,
+// N 256, K 16). CTA r of the pair holds rows [128 r, 128 r + 128) of the A
+// tile and rows [128 r, 128 r + 128) of the B tile (three slices each, K
+// blocks of 64, two stages) and receives output rows [128 r, 128 r + 128) in
+// its own TMEM (2 x 256 columns). The MMA reads each CTA's B half once for
+// both SMs, so a CTA's shared memory serves 64 B per clock of operands at the
+// full MMA rate instead of the 128 B per clock of the single-CTA 128 x 128
+// tile, which is bound by shared-memory bandwidth.
+//
+// Roles: lane 0 of warp 0 in each CTA loads that CTA's halves, signalling the
+// full barrier of CTA 0, whose producer posts the byte count of both; lane 0
+// of warp 1 of CTA 0 issues every MMA and commits to the stage-empty and
+// accumulator-full barriers of both CTAs at once; the eight epilogue warps of
+// each CTA drain their TMEM half and arrive on CTA 0's accumulator-empty
+// barrier. Every wait is bounded as in k_gemm_tc_persist.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// shared::cluster address of the same shared variable in CTA `rank`
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(dst_smem), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// TMA load into this CTA's shared memory whose completion is counted on an
+// mbarrier of either CTA of the pair (bar: shared::cluster address)
+__device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                                 uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+      "%4}], [%5];\n" ::"r"(dst),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+// BF16 x BF16 -> F32, both K-major, M = 256 over the pair, N = 256.
+constexpr uint32_t kIdescPair = (1u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}\n" ::"r"(
+          tmem_d),
+      "l"(da), "l"(db), "r"(kIdescPair), "r"(accumulate), "r"(0)
+      : "memory");
+}
+// commit of this thread's MMAs, arriving on the barrier at the same offset in
+// both CTAs of the pair
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
+          bar),
+      "h"((uint16_t)3)
+      : "memory");
+}
+
+constexpr int kPairBK = 64, kPairS = 2;
+constexpr int kPairAB = 128 * kPairBK * 2;                 // one slice of this CTA's A half
+constexpr int kPairSB = 6 * kPairAB;                       // three A and three B slice halves
+constexpr int kPairSmem = kPairS * kPairSB + kPEpi + 1024 + kPBars;
+static_assert(kPairSmem <= 232448, "CTA-pair GEMM shared memory above the per-CTA limit");
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    k_gemm_tc_pair(const TcDesc* __restrict__ descs, const TcWork* __restrict__ work, int nwork,
+                   int* __restrict__ status, const unsigned long long* __restrict__ wait_ns) {
+  constexpr int S = kPairS, BK = kPairBK, AB = kPairAB, SB = kPairSB;
+  constexpr uint32_t TCOLS = 512;  // double-buffered 256-column FP32 accumulator
+  static_assert((2 * S + 5) * 8 + 4 <= kPBars, "barrier area");
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float* stg_all = reinterpret_cast<float*>(smem + S * SB);
+  // full[S] empty[S] accf[2] acce[2] probe, then the TMEM address
+  uint64_t* bars = (uint64_t*)(smem + S * SB + kPEpi);
+  uint32_t* tmem_slot = (uint32_t*)(smem + S * SB + kPEpi + (2 * S + 5) * 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t rank = cluster_rank();
+  const bool lead = rank == 0;
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[S]);
+  const uint32_t accf0 = smem_u32(&bars[2 * S]), acce0 = smem_u32(&bars[2 * S + 2]);
+  const uint32_t probe = smem_u32(&bars[2 * S + 4]);
+  const uint64_t lim = wait_ns[0];
+  if (warp == 0) tmem_alloc_pair(smem_u32(tmem_slot), TCOLS);
+  if (tid == 0) {
+    for (int b = 0; b < 2 * S + 2; b++) mbar_init(smem_u32(&bars[b]), 1);
+    // accumulator-empty: one arrival per epilogue warp of both CTAs (used in CTA 0)
+    for (int b = 2 * S + 2; b < 2 * S + 4; b++) mbar_init(smem_u32(&bars[b]), 2 * kPEpiWarps);
+    mbar_init(probe, 1);  // probe: nothing ever arrives on it
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  cluster_sync_all();  // both CTAs' barriers initialised before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int G = gridDim.x >> 1;
+  const int cl = blockIdx.x >> 1;
+  bool to = false;
+  if (wait_ns[1] != 0 && (tid == 0 || tid == 32 || warp >= 2)) {
+    if (!mbar_wait(probe, 0, lim)) {
+      report_timeout(status, 5, 0);
+      to = true;
+    }
+  }
+
+  if (tid == 0) {  // TMA producer of this CTA's halves
+    int g = 0;
+    for (int w = cl; w < nwork && !to; w += G) {
+      const TcDesc& d = descs[work[w].desc];
+      const int tile = work[w].tile;
+      const int tm2 = (d.M + 255) / 256;
+      const int m0 = (tile % tm2) * 256 + 128 * (int)rank, n0 = (tile / tm2) * 256 + 128 * (int)rank;
+      const int nk = d.Kp / BK;
+      const int ns = d.nprod == 3 ? 2 : 3;
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g % S;
+        if (g >= S && !mbar_spin(empty0 + 8 * s, ((g / S) + 1) & 1, lim)) { report_timeout(status, 1, g); to = true; break; }
+        const uint32_t fb = map_to_rank(full0 + 8 * s, 0);
+        if (lead) mbar_expect_tx(full0 + 8 * s, 2 * ns * 2 * AB);
+        const uint32_t st = sbase + s * SB;
+        for (int t = 0; t < ns; t++) tma_load_3d_pair(st + t * AB, &d.mapA, kb * BK, m0, t, fb);
+        for (int t = 0; t < ns; t++) tma_load_3d_pair(st + (3 + t) * AB, &d.mapB, kb * BK, n0, t, fb);
+      }
+    }
+    // Drain: a stage's loads have landed once the MMAs that read it have
+    // completed, which its empty barrier records (in both CTAs).
+    for (int gi = g - 1; gi >= 0 && gi >= g - S; gi--)
+      if (!mbar_spin(empty0 + 8 * (gi % S), (gi / S) & 1, kDrainLimitNs)) atomicOr(status, 4);
+  } else if (tid == 32 && lead) {  // MMA issuer of the pair
+    constexpr int pa[6] = {0, 0, 1, 0, 1, 2};
+    constexpr int pb[6] = {0, 1, 0, 2, 1, 0};
+    const uint64_t d0 = smem_desc_kmajor<BK>(sbase);
+    int g = 0, t = 0;
+    uint32_t last_bar = 0, last_par = 0;
+    for (int w = cl; w < nwork && !to; w += G, t++) {
+      const int a = t & 1, u = t >> 1;
+      if (t >= 2 && !mbar_spin(acce0 + 8 * a, (u - 1) & 1, lim)) { report_timeout(status, 2, t); to = true; break; }
+      tc_fence_after();
+      const TcDesc& d = descs[work[w].desc];
+      const int nk = d.Kp / BK;
+      const int np = d.nprod == 3 ? 3 : 6;
+      const uint32_t acc = tmem + a * 256;
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g % S;
+        if (!mbar_spin(full0 + 8 * s, (g / S) & 1, lim)) { report_timeout(status, 3, g); to = true; break; }
+        tc_fence_after();
+        const uint64_t ds = d0 + (uint64_t)((uint32_t)(s * SB) >> 4);
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+          if (p >= np) break;
+#pragma unroll
+          for (int k16 = 0; k16 < BK / 16; k16++)
+            umma_bf16_pair(acc, ds + (uint64_t)((pa[p] * AB + k16 * 32) >> 4),
+                           ds + (uint64_t)(((3 + pb[p]) * AB + k16 * 32) >> 4), (kb > 0 || p > 0 || k16 > 0) ? 1u : 0u);
+        }
+        umma_commit_pair(empty0 + 8 * s);
+        last_bar = empty0 + 8 * s;
+        last_par = (g / S) & 1;
+      }
+      if (!to) {
+        umma_commit_pair(accf0 + 8 * a);
+        last_bar = accf0 + 8 * a;
+        last_par = u & 1;
+      }
+    }
+    if (last_bar && !mbar_spin(last_bar, last_par, kDrainLimitNs)) atomicOr(status, 4);
+  } else if (warp >= 2) {  // epilogue warps of this CTA's 128 rows
+    const int q = warp & 3;
+    constexpr int CH = 256 / 64;
+    const int c0 = ((warp - 2) >> 2) * CH;
+    float* stg = stg_all + (warp - 2) * (32 * 33);
+    const uint32_t acce_lead = map_to_rank(acce0, 0);
+    int t = 0;
+    for (int w = cl; w < nwork && !to; w += G, t++) {
+      const int a = t & 1, u = t >> 1;
+      if (!mbar_wait(accf0 + 8 * a, u & 1, lim)) { report_timeout(status, 4, t); to = true; break; }
+      tc_fence_after();
+      const TcDesc& d = descs[work[w].desc];
+      const int tile = work[w].tile;
+      const int tm2 = (d.M + 255) / 256;
+      const int m0 = (tile % tm2) * 256 + 128 * (int)rank, n0 = (tile / tm2) * 256;
+      const int r0 = m0 + 32 * q;
+      tc_epilogue(d, n0, tmem + a * 256 + ((uint32_t)(32 * q) << 16), r0, lane, stg, c0, c0 + CH);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(acce_lead + 8 * a);
+    }
+  }
+  __syncwarp();
+  __syncthreads_or(to);
+  tc_fence_before();
+  cluster_sync_all();  // both CTAs done with TMEM and with each other's barriers
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc_pair(tmem, TCOLS);
+}
+
+// ---------------------------------------------------------------------------
 // FP64 source / residual assembly, split into row-major BF16 slices [i][j]
 // through a 32x32 shared-memory transpose.
 enum ResKind { RES_NONE = 0, RES_LAP = 1, RES_AOP = 2 };
@@ -547,30 +762,24 @@ struct PrepDesc {
   const double* x0;       // residual: v - R(x0), or null
   int res;                // RES_LAP: R = C^T C ; RES_AOP: R = I + nu C^T C
   double nu;
-  const double* om;       // CN rhs: v += om - nu_cn * C^T C om (or null)
-  double nu_om;
   bf16* Xs;               // 3 slices [i][j], row stride ld, slice stride sX
   long long sX;
   int ld;
-  double* out64;          // optional FP64 copy of v (column-major), or null
 };
 
-__device__ __forceinline__ double lap5(const double* __restrict__ x, int i, int j, int M, int N) {
-  // (C^T C x)(i,j) = 4x - x(i+-1) - x(j+-1), zero outside (0-based i<M, j<N)
-  double c = x[i + (size_t)j * M];
-  double s = 4.0 * c;
-  if (i > 0) s -= x[i - 1 + (size_t)j * M];
-  if (i + 1 < M) s -= x[i + 1 + (size_t)j * M];
-  if (j > 0) s -= x[i + (size_t)(j - 1) * M];
-  if (j + 1 < N) s -= x[i + (size_t)(j + 1) * M];
-  return s;
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 
 // One 32 x 32 tile of one descriptor per block (block map entry {desc, tile},
-// tiles numbered i-fastest). v is assembled column-major (a warp reads 32
-// consecutive i), staged in shared memory, and written row-major as three BF16
-// slices, four consecutive j per thread (8-byte stores; a warp writes four
-// 64-byte row segments per slice).
+// tiles numbered i-fastest). The pass is bound by the bytes in flight, so each
+// block first issues its whole input as asynchronous 8-byte copies into
+// shared memory -- the source tile and, for a residual, x0 with a one-node
+// halo (zero outside the grid, which drops the stencil's boundary terms
+// exactly) -- and waits once. v is then assembled column-major (a warp reads
+// 32 consecutive i) in place and written row-major as three BF16 slices, four
+// consecutive j per thread (8-byte stores; a warp writes four 64-byte row
+// segments per slice).
 __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__ descs,
                                                     const int2* __restrict__ bmap) {
   const int2 bm = bmap[blockIdx.x];
@@ -579,27 +788,54 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
   const int ti = (M + 31) / 32;
   const int i0 = (bm.y % ti) * 32, j0 = (bm.y / ti) * 32;
   __shared__ double t[32][33];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  for (int jj = ty; jj < 32; jj += 8) {
-    int i = i0 + tx, j = j0 + jj;
-    double v = 0.0;
-    if (i < M && j < N) {
-      size_t o = i + (size_t)j * M;
-      v = d.src_scale * d.src[o];
-      if (d.om) v = v + (d.om[o] - d.nu_om * lap5(d.om, i, j, M, N));
+  __shared__ double h[34][35];  // x0(i0 - 1 + a, j0 - 1 + b) at [b][a]
+  const double* x0 = d.x0;
+  for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+    const int a = e & 31, b = e >> 5, i = i0 + a, j = j0 + b;
+    if (i < M && j < N) cp_async8(&t[b][a], d.src + i + (size_t)j * M);
+    else t[b][a] = 0.0;
+  }
+  if (x0) {
+    for (int e = threadIdx.x; e < 34 * 34; e += 256) {
+      const int a = e % 34, b = e / 34, i = i0 - 1 + a, j = j0 - 1 + b;
+      if (i >= 0 && i < M && j >= 0 && j < N) cp_async8(&h[b][a], x0 + i + (size_t)j * M);
+      else h[b][a] = 0.0;
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  // each thread walks four consecutive rows of one column, keeping the x0
+  // column values the next row shares in registers
+  const int tx = threadIdx.x & 31, lb0 = 4 * (threadIdx.x >> 5);
+  const int ic = i0 + tx;
+  double dn = x0 ? h[lb0][tx + 1] : 0.0, c = x0 ? h[lb0 + 1][tx + 1] : 0.0;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int jj = lb0 + r, j = j0 + jj;
+    const double up = x0 ? h[jj + 2][tx + 1] : 0.0;
+    if (ic < M && j < N) {
+      double v = d.src_scale * t[jj][tx];
       if (d.bcsrc) {
-        int a = i + 1, b = j + 1;
+        const int a = ic + 1, b = j + 1;
         if (a == 1 || a == M || b == 1 || b == N)
           v = apply_bc_at(v, a, b, d.m, d.n, 1.0,
                           [&](int side, int I) { return getbc_raw(d.bcsrc, d.m, d.n, side, I) * 1.0; });
       }
-      if (d.out64) d.out64[o] = v;
-      if (d.x0) {
-        double ax = d.res == RES_LAP ? lap5(d.x0, i, j, M, N) : d.x0[o] + d.nu * lap5(d.x0, i, j, M, N);
+      if (x0) {
+        // (C^T C x0)(i,j) = 4 x0 - x0(i+-1) - x0(j+-1), zero outside
+        double s = 4.0 * c;
+        s -= h[jj + 1][tx];
+        s -= h[jj + 1][tx + 2];
+        s -= dn;
+        s -= up;
+        const double ax = d.res == RES_LAP ? s : c + d.nu * s;
         v = v - ax;
       }
+      t[jj][tx] = v;
     }
-    t[jj][tx] = v;
+    dn = c;
+    c = up;
   }
   __syncthreads();
   const int ii = threadIdx.x >> 3, g = threadIdx.x & 7;  // row ii, columns 4g .. 4g+3
@@ -656,7 +892,7 @@ struct PrecisionPlan {
   std::map<int, float*> lam;                        // N+1 -> 1-D eigenvalues
   int* status = nullptr;
   unsigned long long* wait_ns = nullptr;  // device words: limit of the GEMM's waits (ns), probe flag
-  int tc_tile = 0;                        // tile configuration: 0 = the measured autotuner, 1..3
+  int tc_tile = 0;                        // tile configuration: 0 = the measured autotuner, 1..4
   int refine_slices = 0;                  // slices per operand of the correction solves: 0 = by kind, 2 or 3
   int poisson_sweeps = 1;                 // correction sweeps of the Poisson (ctci) solves: 1 or 2
   std::vector<int> tile_choice;           // configuration of each GEMM launch group, in build order
@@ -665,6 +901,7 @@ struct PrecisionPlan {
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 static int g_num_sms = 0;
+static int g_pair_clusters = 0;  // CTA pairs of k_gemm_tc_pair resident at once (0: configuration 4 unavailable)
 
 static inline int rup(int x, int a) { return (x + a - 1) / a * a; }
 
@@ -743,7 +980,8 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
         cudaFuncSetAttribute(k_gemm_tc_persist<256, 32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              tc_smem<256, 32, 2>()) != cudaSuccess ||
         cudaFuncSetAttribute(k_gemm_tc_persist<128, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tc_smem<128, 32, 4>()) != cudaSuccess) {
+                             tc_smem<128, 32, 4>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmem) != cudaSuccess) {
       g_perr = "cannot raise shared memory limit for the tensor-core GEMM";
       return 4;
     }
@@ -751,6 +989,23 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute la[1];
+    la[0].id = cudaLaunchAttributeClusterDimension;
+    la[0].val.clusterDim.x = 2;
+    la[0].val.clusterDim.y = 1;
+    la[0].val.clusterDim.z = 1;
+    lc.gridDim = dim3(2 * std::max(1, g_num_sms / 2));
+    lc.blockDim = dim3(kPThreads);
+    lc.dynamicSmemBytes = kPairSmem;
+    lc.attrs = la;
+    lc.numAttrs = 1;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, k_gemm_tc_pair, &lc) != cudaSuccess) {
+      cudaGetLastError();
+      nc = 0;
+    }
+    g_pair_clusters = nc;
   }
   pp->status = cases.empty() ? (int*)alloc(sizeof(int) * 4) : cases[0].status;
   pp->wait_ns = (unsigned long long*)alloc(2 * sizeof(unsigned long long));
@@ -773,8 +1028,8 @@ int precision_init(PrecisionPlan*& pp, cudaStream_t, const std::vector<DevCase>&
   }
   for (auto& c : cases) {
     CaseBufs b{};
-    // T is the B operand of the left GEMMs: rows padded to the widest tile
-    int Rm = rup(c.m - 1, 128), Rn = rup(c.n - 1, 256), Km = rup(c.m - 1, 64), Kn = rup(c.n - 1, 64);
+    // rows of X and T padded to the widest tile (256)
+    int Rm = rup(c.m - 1, 256), Rn = rup(c.n - 1, 256), Km = rup(c.m - 1, 64), Kn = rup(c.n - 1, 64);
     b.sX = (long long)Rm * Kn;
     b.sT = (long long)Rn * Km;
     b.ldX = Kn;
@@ -841,17 +1096,18 @@ static T* upload(PrecisionPlan* pp, const std::vector<T>& v) {
   return p;
 }
 
-// Output tile width of a tile configuration (1..3, see TcShape above).
-static inline int tc_bn(int cfg) { return cfg == 2 ? 256 : 128; }
+// Output tile of a tile configuration (1..4, see kTcCfgs above).
+static inline int tc_bn(int cfg) { return cfg == 2 || cfg == 4 ? 256 : 128; }
+static inline int tc_bm(int cfg) { return cfg == 4 ? 256 : 128; }
 
 // Work list of one launch group for tile configuration cfg: every tile of
 // every descriptor, sorted by K length (longest first) for balance across the
-// SMs.
+// SMs (across the CTA pairs for configuration 4).
 static std::vector<TcWork> tc_work(const std::vector<TcDesc>& ds, int cfg) {
-  const int bn = tc_bn(cfg);
+  const int bn = tc_bn(cfg), bm = tc_bm(cfg);
   std::vector<TcWork> wl;
   for (int i = 0; i < (int)ds.size(); i++) {
-    const int tiles = ds[i].tiles_m * ((ds[i].N + bn - 1) / bn);
+    const int tiles = ((ds[i].M + bm - 1) / bm) * ((ds[i].N + bn - 1) / bn);
     for (int t = 0; t < tiles; t++) wl.push_back({i, t});
   }
   std::stable_sort(wl.begin(), wl.end(), [&](const TcWork& x, const TcWork& y) { return ds[x.desc].Kp > ds[y.desc].Kp; });
@@ -860,6 +1116,12 @@ static std::vector<TcWork> tc_work(const std::vector<TcDesc>& ds, int cfg) {
 
 static void launch_tc(int cfg, const TcDesc* dd, const TcWork* dw, int nw, int* status,
                       const unsigned long long* wait_ns, cudaStream_t st) {
+  if (cfg == 4) {
+    // one CTA pair per two SMs, at most as many pairs as fit at once
+    const int pairs = std::max(1, std::min(nw, g_pair_clusters));
+    k_gemm_tc_pair<<<2 * pairs, kPThreads, kPairSmem, st>>>(dd, dw, nw, status, wait_ns);
+    return;
+  }
   const int grid = std::min(nw, g_num_sms > 0 ? g_num_sms : 148);
   if (cfg == 2)
     k_gemm_tc_persist<256, 32, 2><<<grid, kPThreads, tc_smem<256, 32, 2>(), st>>>(dd, dw, nw, status, wait_ns);
@@ -921,10 +1183,12 @@ static int tune_tc(PrecisionPlan* pp, const std::vector<TcDesc>& ds, cudaStream_
     cudaMemcpy(dd, t.data(), sizeof(TcDesc) * t.size(), cudaMemcpyHostToDevice);
     float best_ms = 1e30f;
     for (int cfg = 1; cfg <= kTcCfgs; cfg++) {
+      if (cfg == 4 && g_pair_clusters == 0) continue;
       const std::vector<TcWork> wl = tc_work(ds, cfg);
       cudaMemcpy(dw, wl.data(), sizeof(TcWork) * wl.size(), cudaMemcpyHostToDevice);
       const int nw = (int)wl.size();
       launch_tc(cfg, dd, dw, nw, pp->status, pp->wait_ns, st);  // warm-up
+      if (cudaGetLastError() != cudaSuccess) continue;  // a configuration that cannot launch here is not timed
       cudaEventRecord(e0, st);
       for (int r = 0; r < 3; r++) launch_tc(cfg, dd, dw, nw, pp->status, pp->wait_ns, st);
       cudaEventRecord(e1, st);
@@ -950,7 +1214,8 @@ static int tune_tc(PrecisionPlan* pp, const std::vector<TcDesc>& ds, cudaStream_
 // configuration the handle's option or the autotuner chose.
 static void add_gemm_persist(PrecisionPlan* pp, Prog& P, const std::vector<TcDesc>& ds, cudaStream_t st) {
   if (ds.empty()) return;
-  const int cfg = pp->tc_tile >= 1 && pp->tc_tile <= kTcCfgs ? pp->tc_tile : tune_tc(pp, ds, st);
+  int cfg = pp->tc_tile >= 1 && pp->tc_tile <= kTcCfgs ? pp->tc_tile : tune_tc(pp, ds, st);
+  if (cfg == 4 && g_pair_clusters == 0) cfg = 1;  // no CTA pair fits on this device
   pp->tile_choice.push_back(cfg);
   std::vector<TcWork> wl = tc_work(ds, cfg);
   double fl = 0.0;
@@ -1008,7 +1273,6 @@ static void build_solves(PrecisionPlan* pp, Prog& P, std::vector<SolveReq>& rq, 
       PrepDesc pd = r.src;
       pd.m = c.m; pd.n = c.n;
       pd.Xs = b.Xs; pd.sX = b.sX; pd.ld = b.ldX;
-      pd.out64 = nullptr;
       if (pass >= 1) {
         pd.x0 = r.out;
         pd.res = r.fkind == F_LAMINV ? RES_LAP : RES_AOP;
@@ -1068,11 +1332,10 @@ void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, co
       // b = norm*rhsA + (I - nu_k C^T C) omega_k ; omega_k <- A_k^-1 b
       SolveReq r{};
       r.c = (int)i; r.hc = &cs[i]; r.k = k; r.fkind = F_LAM1I_NORM;
-      double* om = c.omega + (size_t)(k - 1) * c.ns;
-      r.src.src = c.rhsA; r.src.src_scale = c.norm;
-      r.src.om = om;
-      r.src.nu_om = 0.5 * c.dt / (c.delta * c.delta * std::pow(4.0, k - 1) * c.re);
-      r.out = om;
+      r.out = c.omega + (size_t)(k - 1) * c.ns;
+      // the correction residual's right-hand side is b itself (wd)
+      r.src.src = c.wd; r.src.src_scale = 1.0;
+      r.presplit = true;
       rq.push_back(r);
     }
     // b = norm*rhsA + (I - nu_k C^T C) omega_k is assembled once, in the same
@@ -1085,12 +1348,10 @@ void build_precision_step1(PrecisionPlan* pp, Prog& P, const DevCase* dcases, co
       SolveReq& r = rq[q];
       const DevCase& c = *r.hc;
       const CaseBufs& b = pp->bufs[r.c];
-      sd.push_back({c.norm, r.src.nu_om, c.wd, reinterpret_cast<uint16_t*>(b.Xs), b.sX, b.ldX});
+      const double nu = 0.5 * c.dt / (c.delta * c.delta * std::pow(4.0, r.k - 1) * c.re);
+      sd.push_back({c.norm, nu, c.wd, reinterpret_cast<uint16_t*>(b.Xs), b.sX, b.ldX});
       const int tiles = ((c.m - 1 + 31) / 32) * ((c.n - 1 + 31) / 32);
       for (int t = 0; t < tiles; t++) tmap.push_back(make_int2((int)q, t));
-      r.src = PrepDesc{};
-      r.src.src = c.wd; r.src.src_scale = 1.0;
-      r.presplit = true;
     }
     LevelItem* d_it = upload(pp, it);
     const RhsSplitDesc* d_sd = upload(pp, sd);

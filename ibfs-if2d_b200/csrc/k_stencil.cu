@@ -142,9 +142,13 @@ __global__ void __launch_bounds__(256) k_rhs(const DevCase* __restrict__ cases, 
 // the diffusion applied by the 5-point stencil), written as FP64 (the
 // refinement residual's right-hand side) and as three BF16 slices, row-major,
 // through a shared-memory transpose. rhs_old = rhs as in k_rhs; rhsA itself
-// is never stored. The kernel is latency-bound: four resident blocks per SM
-// (at most 64 registers a thread) measured 0.45 ms per step faster on the
-// 256-case batch than the three that 78 registers allow.
+// is never stored.
+//
+// The kernel streams ~54 bytes per node and is bound by how many of them are
+// in flight: each block first issues its whole input as asynchronous 8-byte
+// copies into shared memory (omega with a one-node halo, the u and v faces
+// the flux averages read, rhs_old), waits once, and then computes from shared
+// memory. Four resident blocks per SM (at most 64 registers a thread).
 __device__ __forceinline__ double lap5_nodes(const double* __restrict__ x, int i, int j, int M, int N) {
   double c = x[i + (size_t)j * M];
   double s = 4.0 * c;
@@ -166,6 +170,37 @@ __device__ __forceinline__ void split3_bf16(double x, uint16_t& s0, uint16_t& s1
   s2 = __bfloat16_as_ushort(c);
 }
 
+__device__ __forceinline__ void cp_async8(void* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Stage a rows x cols window (origin r0, c0) of a column-major field with
+// leading dimension ld and extents R x Cn into s[col][row] (row stride SP);
+// entries outside the field are zero.
+template <int SP>
+__device__ __forceinline__ void stage_window(double* s, const double* __restrict__ f, int ld, int R, int Cn, int r0,
+                                             int c0, int rows, int cols) {
+  for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
+    const int a = e % rows, b = e / rows, r = r0 + a, c = c0 + b;
+    double* d = s + b * SP + a;
+    if (r >= 0 && r < R && c >= 0 && c < Cn) cp_async8(d, f + r + (size_t)c * ld);
+    else *d = 0.0;
+  }
+}
+
+struct RhsTile {
+  double om[34][35];  // omega(i0 - 1 + a, j0 - 1 + b) at [b][a] (node coordinates, 0-based)
+  double u[33][35];   // u face (i0 + a, j0 + b) at [b][a], a < 34 (face coordinates, 0-based)
+  double v[34][34];   // v face (i0 + a, j0 + b) at [b][a], a < 33
+  double t[32][33];   // rhs_old, then the assembled b
+};
+
 __global__ void __launch_bounds__(256, 4) k_rhs_split(const DevCase* __restrict__ cases,
                                                    const LevelItem* __restrict__ items,
                                                    const RhsSplitDesc* __restrict__ sd,
@@ -174,24 +209,114 @@ __global__ void __launch_bounds__(256, 4) k_rhs_split(const DevCase* __restrict_
   const LevelItem it = items[bm.x];
   const RhsSplitDesc& d = sd[bm.x];
   const DevCase& C = cases[it.c];
-  const int M = C.m - 1, N = C.n - 1;
+  const int m = C.m, n = C.n, M = m - 1, N = n - 1, k = it.k;
   const int ti = (M + 31) / 32;
   const int i0 = (bm.y % ti) * 32, j0 = (bm.y / ti) * 32;
-  const double* om = C.omega + (size_t)(it.k - 1) * C.ns;
-  __shared__ double tile[32][33];
+  const double* om = C.omega + (size_t)(k - 1) * C.ns;
+  __shared__ RhsTile S;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  const bool q0c = C.q0_const != 0;
-  for (int jj = ty; jj < 32; jj += 8) {
-    const int i = i0 + tx, j = j0 + jj;
-    double v = 0.0;
-    if (i < M && j < N) {
-      const int t = i + j * M;
-      const double rA = q0c ? rhs_value<true>(C, it, t, first_step) : rhs_value<false>(C, it, t, first_step);
-      v = d.scale * rA;
-      v = v + (om[t] - d.nu * lap5_nodes(om, i, j, M, N));
-      d.b64[t] = v;
+  if (!C.q0_const) {
+    // general q0: direct loads
+    for (int jj = ty; jj < 32; jj += 8) {
+      const int i = i0 + tx, j = j0 + jj;
+      double v = 0.0;
+      if (i < M && j < N) {
+        const int t = i + j * M;
+        const double rA = rhs_value<false>(C, it, t, first_step);
+        v = d.scale * rA;
+        v = v + (om[t] - d.nu * lap5_nodes(om, i, j, M, N));
+        d.b64[t] = v;
+      }
+      S.t[jj][tx] = v;
     }
-    tile[jj][tx] = v;
+  } else {
+    const double* q = C.q + (size_t)(k - 1) * C.nq;
+    const double* qv = q + (size_t)(m + 1) * n;
+    double* ro = C.rhs_old + (size_t)(k - 1) * C.ns;
+    const bool euler = first_step || *C.itime == 1;
+    stage_window<35>(&S.om[0][0], om, M, M, N, i0 - 1, j0 - 1, 34, 34);
+    stage_window<35>(&S.u[0][0], q, m + 1, m + 1, n, i0, j0, 34, 33);
+    stage_window<34>(&S.v[0][0], qv, m, m, n + 1, i0, j0, 33, 34);
+    if (!euler) stage_window<33>(&S.t[0][0], ro, M, M, N, i0, j0, 32, 32);
+    cp_async_all();
+    __syncthreads();
+    const double u0 = C.q0_u1 * (double)(1 << (k - 1));
+    const double* bc = C.lastbc + (size_t)(k - 1) * C.nring;
+    const int bottom = 2 * (n + 1), top = 2 * (n + 1) + m + 1, right = n + 1;
+    const double del22 = C.delta * C.delta * (double)(1 << (2 * (k - 1)));
+    const double vf = 0.5 * C.dt / C.re / del22 / C.norm;
+    const double con1 = 1.5 * C.dt / del22 / C.norm;
+    const double con2 = -0.5 * C.dt / del22 / C.norm;
+    // Each thread walks four consecutive rows of one column of the tile and
+    // keeps the values its next row shares with this one (the omega column,
+    // the lower u faces, the v-face averages and fqu(j)) in registers. The
+    // nonlinear term follows the reference's order (operators.f90:465-510,
+    // :291-304) with q0 in closed form, as rhs_value<true>.
+    const int la = tx, lb0 = 4 * ty;
+    const int i = i0 + la + 2;  // reference (1-based) node index
+    const bool iok = i - 2 < M;
+    auto vrow = [&](int b) { return 0.5 * (S.v[b][la + 1] + S.v[b][la] + 0.0 + 0.0); };  // vavg(i, j0 + b + 1)
+    double dn = S.om[lb0][la + 1], c = S.om[lb0 + 1][la + 1];
+    double ul0 = S.u[lb0][la], ul1 = S.u[lb0][la + 1], ul2 = S.u[lb0][la + 2];
+    double vb0 = vrow(lb0), vb1 = vrow(lb0 + 1);
+    double fq_lo = 0.0;  // fqu(j - 1) = 0.5 (vavg(j) Wj(j) + vavg(j-1) Wj(j-1))
+    {
+      const int j = j0 + lb0 + 2;
+      if (iok && j - 2 < N) fq_lo = 0.5 * (vb1 * c + vb0 * (j - 1 == 1 ? bc[bottom + i - 1] : dn));
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int lb = lb0 + r, j = j0 + lb + 2;
+      const double up = S.om[lb + 2][la + 1], L = S.om[lb + 1][la], R = S.om[lb + 1][la + 2];
+      const double uh0 = S.u[lb + 1][la], uh1 = S.u[lb + 1][la + 1], uh2 = S.u[lb + 1][la + 2];
+      const double vb2 = vrow(lb + 2);
+      if (!iok || j - 2 >= N) {
+        S.t[lb][la] = 0.0;  // the K padding of the slices reads zero
+      } else {
+        const double WjU = j + 1 == n + 1 ? bc[top + i - 1] : up;
+        const double fq_hi = 0.5 * (vb2 * WjU + vb1 * c);  // fqu(j)
+        const double WiL = i - 1 == 1 ? bc[j - 1] : L;
+        const double WiR = i + 1 == m + 1 ? bc[right + j - 1] : R;
+        const double ua_m = 0.5 * (uh0 + ul0 + u0 + u0);  // uavg(i-1, j)
+        const double ua_c = 0.5 * (uh1 + ul1 + u0 + u0);  // uavg(i, j)
+        const double ua_p = 0.5 * (uh2 + ul2 + u0 + u0);  // uavg(i+1, j)
+        const double fqv_i = -0.5 * (ua_p * WiR + ua_c * c);
+        const double fqv_im = -0.5 * (ua_c * c + ua_m * WiL);
+        const double rhs = fqv_i - fqv_im - fq_hi + fq_lo;
+        fq_lo = fq_hi;
+        const double rold = euler ? rhs : S.t[lb][la];
+        const int a = i - 1, b = j - 1;
+        double rb = 0.0;
+        if (a == 1 || a == m - 1 || b == 1 || b == n - 1) {
+          rb = apply_bc_at(rb, a, b, m, n, vf, [&](int side, int I) { return ring_at(bc, m, n, side, I); });
+          if (k < C.L) {
+            const double* cr = C.omega + (size_t)k * C.ns;  // omega_{k+1}, already advanced
+            rb = apply_bc_at(rb, a, b, m, n, vf,
+                             [&](int side, int I) { return getbc_raw(cr, m, n, side, I) * 0.25; });
+          } else {
+            rb = apply_bc_at(rb, a, b, m, n, vf, [&](int, int) { return 0.0; });
+          }
+        }
+        const int t = (i - 2) + (j - 2) * M;
+        ro[t] = rhs;
+        const double rA = con1 * rhs + con2 * rold + rb;
+        // 5-point stencil of omega; the zero halo outside the grid drops the
+        // boundary terms exactly as lap5_nodes does
+        double s = 4.0 * c;
+        s -= L;
+        s -= R;
+        s -= dn;
+        s -= up;
+        double v = d.scale * rA;
+        v = v + (c - d.nu * s);
+        d.b64[t] = v;
+        S.t[lb][la] = v;
+      }
+      dn = c;
+      c = up;
+      ul0 = uh0; ul1 = uh1; ul2 = uh2;
+      vb1 = vb2;
+    }
   }
   __syncthreads();
   const int ii = threadIdx.x >> 3, g = threadIdx.x & 7;  // row ii, columns 4g .. 4g+3
@@ -199,7 +324,7 @@ __global__ void __launch_bounds__(256, 4) k_rhs_split(const DevCase* __restrict_
   if (i < M && j < N) {
     uint16_t a[4], b[4], c[4];
 #pragma unroll
-    for (int e = 0; e < 4; e++) split3_bf16(tile[4 * g + e][ii], a[e], b[e], c[e]);
+    for (int e = 0; e < 4; e++) split3_bf16(S.t[4 * g + e][ii], a[e], b[e], c[e]);
     // row stride and slice stride are multiples of 64 elements: 8-byte aligned
     // groups; columns >= N of the last group are zero (the K padding)
     uint16_t* o = d.Xs + (size_t)i * d.ld + j;
@@ -247,7 +372,7 @@ __global__ void __launch_bounds__(256) k_coarsify(const DevCase* __restrict__ ca
 // ---------------------------------------------------------------------------
 // curl (operators.f90:243-288) of s_k with sbc_k = get_bc(s_{k+1}, 1.0)
 // (operators.f90:231; zero on the coarsest level, :218) into q_k.
-__device__ __forceinline__ void curl_at(const DevCase& C, LevelItem it, int t) {
+__device__ __forceinline__ double curl_value(const DevCase& C, LevelItem it, int t) {
   int m = C.m, n = C.n;
   int k = it.k;
   const double* x = C.s + (size_t)(k - 1) * C.ns;
@@ -271,16 +396,31 @@ __device__ __forceinline__ void curl_at(const DevCase& C, LevelItem it, int t) {
     else if (i == m) v = -xbc(SIDE_RIGHT, j) + x[nidx(m, j, m)];
     else v = x[nidx(i, j, m)] - x[nidx(i + 1, j, m)];
   }
-  C.q[(size_t)(k - 1) * C.nq + t] = v;
+  return v;
 }
 
+// A thread's four faces are all read before any is stored (q and s may not
+// alias, but the compiler cannot know that), so each thread has its loads of
+// the four in flight at once.
 __global__ void __launch_bounds__(256) k_curl(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items,
                                               const int2* __restrict__ bmap) {
+  static_assert(kBlockElems == 4 * 256, "four faces per thread");
   const int2 bm = bmap[blockIdx.x];
   const LevelItem it = items[bm.x];
   const DevCase& C = cases[it.c];
   const int tend = min(C.nq, bm.y + kBlockElems);
-  for (int t = bm.y + (int)threadIdx.x; t < tend; t += 256) curl_at(C, it, t);
+  double v[4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int t = bm.y + (int)threadIdx.x + 256 * r;
+    v[r] = t < tend ? curl_value(C, it, t) : 0.0;
+  }
+  double* q = C.q + (size_t)(it.k - 1) * C.nq;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int t = bm.y + (int)threadIdx.x + 256 * r;
+    if (t < tend) q[t] = v[r];
+  }
 }
 
 // ---------------------------------------------------------------------------

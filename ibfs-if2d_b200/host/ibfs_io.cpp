@@ -196,7 +196,7 @@ bool parse_b200_options(const std::string& text, ibfs_options_c& o, std::string&
     else if (k == "CG_PRECOND") ok = to_logical(v, o.cg_precond) || to_int(v, o.cg_precond);
     else if (k == "REFINE_SLICES") ok = to_int(v, o.refine_slices) && (o.refine_slices == 0 || o.refine_slices == 2 || o.refine_slices == 3);
     else if (k == "POISSON_SWEEPS") ok = to_int(v, o.poisson_sweeps) && o.poisson_sweeps >= 0 && o.poisson_sweeps <= 2;
-    else if (k == "TC_TILE") ok = to_int(v, o.tc_tile) && o.tc_tile >= 0 && o.tc_tile <= 3;
+    else if (k == "TC_TILE") ok = to_int(v, o.tc_tile) && o.tc_tile >= 0 && o.tc_tile <= 4;
     else {
       msg = "unknown &B200_OPTIONS item " + k;
       return false;

@@ -75,8 +75,10 @@ typedef struct {
   int tc_tile;         /* split-precision form: tile configuration of the tensor-core
                           GEMM: 1 = 128x128 output tile, K blocks of 64, two pipeline
                           stages; 2 = 128x256, K blocks of 32, two stages; 3 = 128x128,
-                          K blocks of 32, four stages; 0 = the measured autotuner picks
-                          per launch group. Taken from the first case of a batch   */
+                          K blocks of 32, four stages; 4 = 256x256 on a pair of CTAs
+                          (tcgen05 cta_group::2), K blocks of 64, two stages; 0 = the
+                          measured autotuner picks per launch group. Taken from the
+                          first case of a batch                                    */
   int refine_slices;   /* split-precision form: BF16 slices per operand in the correction
                           solves of the refinement: 0 = three (six products) for the
                           Poisson solves of vort2flux, two (three products) for the
@@ -186,7 +188,7 @@ int ibfs_last_timing(const ibfs_handle* h, double* ms);
  * counterpart; reports the launch structure of the advance). */
 int ibfs_kernels_per_step(const ibfs_handle* h);
 
-/* Tile configurations (1..3, as ibfs_options_c.tc_tile) of the
+/* Tile configurations (1..4, as ibfs_options_c.tc_tile) of the
  * split-precision form's tensor-core GEMM launch groups of the step program,
  * in launch order: writes up to max of them to cfgs (may be NULL) and
  * returns how many there are (0 for a plain FP64 handle). No reference

@@ -48,20 +48,22 @@ def test_precision_advance(body, m, lev, steps):
     assert rel(sg["q"], so["q"]) < 1e-8
 
 
-@pytest.mark.parametrize("m,lev", [(128, 3), (256, 2)])
+@pytest.mark.parametrize("m,lev", [(128, 3), (256, 2), (192, 2), (384, 2)])
 def test_tensor_core_tile_shapes_and_autotuner(m, lev):
-    """The tensor-core GEMM's three tile configurations (128 x 128 with K
+    """The tensor-core GEMM's four tile configurations (128 x 128 with K
     blocks of 64 and two stages; 128 x 256, K 32, two stages; 128 x 128, K 32,
-    four stages) and the measured autotuner's per-launch-group choice all
-    follow the FP64 oracle at the split-precision bar; the tuner reports a
-    configuration for every GEMM launch group of the step."""
+    four stages; 256 x 256 on a CTA pair, K 64, two stages) and the measured
+    autotuner's per-launch-group choice all follow the FP64 oracle at the
+    split-precision bar, including grids whose m - 1 is not a multiple of the
+    tile (191, 383); the tuner reports a configuration for every GEMM launch
+    group of the step."""
     xb, yb = O.line(4.0 / m, 1.0, 30.0)
     oc = O.Case(O.make_params(m, m, 0.004, 300.0, lev), xb, yb)
     for _ in range(4):
         oc.advance()
     ref = oc.get_state()["omega"]
     widths = {}
-    for tile in (1, 2, 3, 0):
+    for tile in (1, 2, 3, 4, 0):
         g = C.Solver(C.make_params(m, m, 0.004, 300.0, lev), (xb, yb), C.make_options(precision=1, tc_tile=tile))
         widths[tile] = g.gemm_tiles()
         g.advance_n(4, want_hist=False)
@@ -69,6 +71,6 @@ def test_tensor_core_tile_shapes_and_autotuner(m, lev):
         x = np.random.default_rng(3).standard_normal(g.sizes[0]["ns"])
         assert rel(g.apply_op(1, x), oc.ctci(x)) < 1e-9, tile
         g.close()
-    for tile in (1, 2, 3):
+    for tile in (1, 2, 3, 4):
         assert widths[tile] and set(widths[tile]) == {tile}
-    assert len(widths[0]) == len(widths[1]) and set(widths[0]) <= {1, 2, 3}
+    assert len(widths[0]) == len(widths[1]) and set(widths[0]) <= {1, 2, 3, 4}
