@@ -579,6 +579,8 @@ def run_ours(args):
     pk, src = peaks()
     cases = W.batch(BATCH["ncases"], seed=SEED)[:args.ncases]
     params, bodies, opts = W.solver_args(cases, C, 1)
+    for o in opts:
+        o.tc_tile = args.tc_tile
     t0 = time.perf_counter()
     g = C.Solver(params, bodies, opts)
     t_create = time.perf_counter() - t0
@@ -847,6 +849,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="headline batch measurement only (no FP64 / plate / adjoint / CPU legs)")
     ap.add_argument("--ref-procs", type=int, default=128)
+    ap.add_argument("--tc-tile", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="tensor-core GEMM tile configuration of the batched form (0: the measured autotuner)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

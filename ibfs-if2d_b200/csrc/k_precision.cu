@@ -263,7 +263,7 @@ __device__ __forceinline__ void store8(bf16* dst, const bf16* v) {
 // Persistent GEMM (k_gemm_tc_persist): one CTA per SM walks
 // a cost-sorted work list of (desc, tile) items. Warp 0 lane 0 issues the TMA
 // loads, warp 1 lane 0 the tcgen05.mma; the accumulator is double-buffered in
-// TMEM (2 x 128 columns) so warps 2-5 drain tile t (tcgen05.ld + epilogue)
+// TMEM (2 x BN columns) so warps 2-9 drain tile t (tcgen05.ld + epilogue)
 // while tile t+1 is loaded and multiplied. Per-tile fixed costs (TMEM
 // allocation, pipeline fill, epilogue) are thereby hidden behind the MMAs.
 struct TcWork {
@@ -871,11 +871,11 @@ __global__ void k_sub(const AxpyDesc* __restrict__ ds) {
 static std::string g_perr;
 
 struct CaseBufs {
-  bf16* Xs;    // 3 slices, rows Rm = roundup(m-1,128), ld = Kn = roundup(n-1,64)
-  bf16* Ts;    // 3 slices, rows Rn = roundup(n-1,128), ld = Km = roundup(m-1,64)
+  bf16* Xs;    // 3 slices, rows Rm = roundup(m-1,256), ld = Kn = roundup(n-1,64)
+  bf16* Ts;    // 3 slices, rows Rn = roundup(n-1,256), ld = Km = roundup(m-1,64)
   long long sX, sT;
   int ldX, ldT;
-  const bf16* Sm;  // sine slices for m: rows roundup(m-1,128), ld roundup(m-1,64)
+  const bf16* Sm;  // sine slices for m: rows roundup(m-1,256), ld roundup(m-1,64)
   const bf16* Sn;
   long long sSm, sSn;
   int ldSm, ldSn;
