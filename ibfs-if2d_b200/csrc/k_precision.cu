@@ -236,12 +236,29 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
-__device__ __forceinline__ void split3f(float x, bf16& s0, bf16& s1, bf16& s2) {
-  s0 = __float2bfloat16_rn(x);
-  float r = x - __bfloat162float(s0);
-  s1 = __float2bfloat16_rn(r);
-  r = r - __bfloat162float(s1);
-  s2 = __float2bfloat16_rn(r);
+// Three-slice split of eight FP32 values (each slice the round-to-nearest
+// BF16 of what the slices before it leave) with packed conversions: one
+// cvt.rn.bf16x2.f32 rounds two values, and the packed words are the store
+// format, so no repacking follows. u0, u1, u2: slices 0, 1, 2 of x[0..7].
+__device__ __forceinline__ uint32_t cvt_bf16x2(float lo, float hi) {
+  __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&p);
+}
+__device__ __forceinline__ float bf16lo(uint32_t p) { return __uint_as_float(p << 16); }
+__device__ __forceinline__ float bf16hi(uint32_t p) { return __uint_as_float(p & 0xffff0000u); }
+__device__ __forceinline__ void split8_packed(const float* x, uint4& u0, uint4& u1, uint4& u2) {
+  uint32_t w0[4], w1[4], w2[4];
+#pragma unroll
+  for (int h = 0; h < 4; h++) {
+    const float a = x[2 * h], b = x[2 * h + 1];
+    w0[h] = cvt_bf16x2(a, b);
+    const float ra = a - bf16lo(w0[h]), rb = b - bf16hi(w0[h]);
+    w1[h] = cvt_bf16x2(ra, rb);
+    w2[h] = cvt_bf16x2(ra - bf16lo(w1[h]), rb - bf16hi(w1[h]));
+  }
+  u0 = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+  u1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+  u2 = make_uint4(w2[0], w2[1], w2[2], w2[3]);
 }
 
 __device__ __forceinline__ void store4(bf16* dst, const bf16* v) {
@@ -249,14 +266,6 @@ __device__ __forceinline__ void store4(bf16* dst, const bf16* v) {
   u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
   u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
   *reinterpret_cast<uint2*>(dst) = u;
-}
-__device__ __forceinline__ void store8(bf16* dst, const bf16* v) {
-  uint4 u;
-  u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
-  u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
-  u.z = (uint32_t)__bfloat16_as_ushort(v[4]) | ((uint32_t)__bfloat16_as_ushort(v[5]) << 16);
-  u.w = (uint32_t)__bfloat16_as_ushort(v[6]) | ((uint32_t)__bfloat16_as_ushort(v[7]) << 16);
-  *reinterpret_cast<uint4*>(dst) = u;
 }
 
 // ---------------------------------------------------------------------------
@@ -335,13 +344,15 @@ __device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t tr
 #pragma unroll 1
         for (int k = 0; k < 4; k++) {
           const int c = seg + 8 * k;
-          bf16 s0[8], s1[8], s2[8];
+          float x[8];
 #pragma unroll
-          for (int e = 0; e < 8; e++) split3f(stg[c * 33 + part * 8 + e], s0[e], s1[e], s2[e]);
+          for (int e = 0; e < 8; e++) x[e] = stg[c * 33 + part * 8 + e];
+          uint4 u0, u1, u2;
+          split8_packed(x, u0, u1, u2);
           bf16* o = Cs + (size_t)(jb + c) * ldcs + r0 + part * 8;
-          store8(o, s0);
-          store8(o + sC, s1);
-          store8(o + 2 * sC, s2);
+          *reinterpret_cast<uint4*>(o) = u0;
+          *reinterpret_cast<uint4*>(o + sC) = u1;
+          *reinterpret_cast<uint4*>(o + 2 * sC) = u2;
         }
       }
       __syncwarp();
@@ -361,13 +372,15 @@ __device__ __forceinline__ void tc_epilogue(const TcDesc& d, int n0, uint32_t tr
 #pragma unroll 1
         for (int k = 0; k < 4; k++) {
           const int rr = seg + 8 * k;
-          bf16 s0[8], s1[8], s2[8];
+          float x[8];
 #pragma unroll
-          for (int e = 0; e < 8; e++) split3f(stg[rr * 33 + part * 8 + e], s0[e], s1[e], s2[e]);
+          for (int e = 0; e < 8; e++) x[e] = stg[rr * 33 + part * 8 + e];
+          uint4 u0, u1, u2;
+          split8_packed(x, u0, u1, u2);
           bf16* o = Cs + (size_t)(r0 + rr) * ldcs + jb + part * 8;
-          store8(o, s0);
-          store8(o + sC, s1);
-          store8(o + 2 * sC, s2);
+          *reinterpret_cast<uint4*>(o) = u0;
+          *reinterpret_cast<uint4*>(o + sC) = u1;
+          *reinterpret_cast<uint4*>(o + 2 * sC) = u2;
         }
       }
       __syncwarp();
