@@ -219,7 +219,8 @@ def roofline_gemm(prof, alg_flops, issued_flops, pk, src):
     ach = alg_flops / secs / 1e12
     peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
     roof = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-            "traffic": None, "kernel": "k_gemm_tc_persist (split-BF16 tcgen05 sine-transform GEMM)",
+            "traffic": None, "kernel": "k_gemm_tc_persist + k_gemm_tc_pair (split-BF16 tcgen05 sine-transform GEMM; "
+                      "single-CTA or CTA-pair tile per launch group, by the autotuner)",
             "peak_source": f"{src} (bf16 sustained)",
             "basis": "algorithmic = (7L+2) DSTs per case-step x 2(m-1)(n-1)[(m-1)+(n-1)] flops, unpadded",
             "launches_per_step": d["launches"], "avg_launch_us": d["ms"] / d["launches"] * 1e3,

@@ -165,6 +165,20 @@ def test_batch_every_size_and_level_count(pool, precision, tol):
               f"omega {max(e['omega']):.2e} force {e['force']:.2e} per step {e['force_per_step']:.2e}")
 
 
+def test_batch_split_form_on_cta_pair_tiles(pool):
+    """The same batch in the split form with every tensor-core GEMM on the
+    256 x 256 CTA-pair tile (tile configuration 4), whose tiles pad m - 1 =
+    127, 191 and 383 to 256 or 512 rows, against the same oracle runs."""
+    params, bodies, opts = W.solver_args(MIX, C, 1)
+    for o in opts:
+        o.tc_tile = 4
+    g = C.Solver(params, bodies, opts)
+    hist = g.advance_n(STEPS["mix"])
+    assert g.gemm_tiles() and set(g.gemm_tiles()) == {4}
+    for i in range(len(MIX)):
+        compare(g, hist, i, pool.get(f"mix{i}"), SPLIT_TOL, SPLIT_STEP_TOL)
+
+
 def test_split_form_long_horizon(pool):
     """The split-precision form stays within 1e-8 of the FP64 oracle over 400
     steps (drag and lift at every step, fields at the end)."""
