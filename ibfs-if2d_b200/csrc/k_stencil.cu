@@ -372,24 +372,19 @@ __global__ void __launch_bounds__(256) k_coarsify(const DevCase* __restrict__ ca
 // ---------------------------------------------------------------------------
 // curl (operators.f90:243-288) of s_k with sbc_k = get_bc(s_{k+1}, 1.0)
 // (operators.f90:231; zero on the coarsest level, :218) into q_k.
-__device__ __forceinline__ double curl_value(const DevCase& C, LevelItem it, int t) {
-  int m = C.m, n = C.n;
-  int k = it.k;
-  const double* x = C.s + (size_t)(k - 1) * C.ns;
-  const double* cs = (k < C.L) ? C.s + (size_t)k * C.ns : nullptr;
+// u face (i, j) (u = true) or v face (i, j) of level k, the reference's
+// expressions in its order; x = s_k, cs = s_{k+1} (null on the coarsest level).
+__device__ __forceinline__ double curl_face(bool u, int i, int j, int m, int n, const double* __restrict__ x,
+                                            const double* __restrict__ cs) {
   auto xbc = [&](int side, int I) -> double { return cs ? getbc_raw(cs, m, n, side, I) * 1.0 : 0.0; };
   double v;
-  int nu = (m + 1) * n;
-  if (t < nu) {
-    int i = t % (m + 1) + 1, j = t / (m + 1) + 1;
+  if (u) {
     if (i == 1) v = xbc(SIDE_LEFT, j + 1) - xbc(SIDE_LEFT, j);
     else if (i == m + 1) v = xbc(SIDE_RIGHT, j + 1) - xbc(SIDE_RIGHT, j);
     else if (j == 1) v = x[nidx(i, 2, m)] - xbc(SIDE_BOTTOM, i);
     else if (j == n) v = xbc(SIDE_TOP, i) - x[nidx(i, n, m)];
     else v = x[nidx(i, j + 1, m)] - x[nidx(i, j, m)];
   } else {
-    int tv = t - nu;
-    int i = tv % m + 1, j = tv / m + 1;
     if (j == 1) v = xbc(SIDE_BOTTOM, i) - xbc(SIDE_BOTTOM, i + 1);
     else if (j == n + 1) v = xbc(SIDE_TOP, i) - xbc(SIDE_TOP, i + 1);
     else if (i == 1) v = -x[nidx(2, j, m)] + xbc(SIDE_LEFT, j);
@@ -399,27 +394,48 @@ __device__ __forceinline__ double curl_value(const DevCase& C, LevelItem it, int
   return v;
 }
 
-// A thread's four faces are all read before any is stored (q and s may not
-// alias, but the compiler cannot know that), so each thread has its loads of
-// the four in flight at once.
+// A thread's four faces (t, t + 256, t + 512, t + 768 of the level's face
+// list: u faces column by column, then v faces) are all read before any is
+// stored, so its loads of the four are in flight at once; the face's (i, j)
+// comes from one division per thread, then by stepping 256 faces at a time.
 __global__ void __launch_bounds__(256) k_curl(const DevCase* __restrict__ cases, const LevelItem* __restrict__ items,
                                               const int2* __restrict__ bmap) {
   static_assert(kBlockElems == 4 * 256, "four faces per thread");
   const int2 bm = bmap[blockIdx.x];
   const LevelItem it = items[bm.x];
   const DevCase& C = cases[it.c];
+  const int m = C.m, n = C.n, k = it.k;
   const int tend = min(C.nq, bm.y + kBlockElems);
+  const int nu = (m + 1) * n;
+  const double* x = C.s + (size_t)(k - 1) * C.ns;
+  const double* cs = (k < C.L) ? C.s + (size_t)k * C.ns : nullptr;
+  int t = bm.y + (int)threadIdx.x;
+  bool u = t < nu;
+  int per = u ? m + 1 : m;
+  int jq = (u ? t : t - nu) / per;
+  int iq = (u ? t : t - nu) - jq * per;
   double v[4];
 #pragma unroll
   for (int r = 0; r < 4; r++) {
-    const int t = bm.y + (int)threadIdx.x + 256 * r;
-    v[r] = t < tend ? curl_value(C, it, t) : 0.0;
+    v[r] = t < tend ? curl_face(u, iq + 1, jq + 1, m, n, x, cs) : 0.0;
+    t += 256;
+    iq += 256;
+    while (iq >= per) {
+      iq -= per;
+      jq++;
+    }
+    if (u && t >= nu) {  // into the v faces
+      u = false;
+      per = m;
+      jq = (t - nu) / per;
+      iq = (t - nu) - jq * per;
+    }
   }
-  double* q = C.q + (size_t)(it.k - 1) * C.nq;
+  double* q = C.q + (size_t)(k - 1) * C.nq;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
-    const int t = bm.y + (int)threadIdx.x + 256 * r;
-    if (t < tend) q[t] = v[r];
+    const int tr = bm.y + (int)threadIdx.x + 256 * r;
+    if (tr < tend) q[tr] = v[r];
   }
 }
 
