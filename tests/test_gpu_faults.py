@@ -6,7 +6,8 @@ traps or hangs the GPU:
   point outside the grid has no faces within the support of its delta kernel,
   so its row and column of A are zero and choldc meets a zero pivot; the oracle
   fails on the same input;
-* a bounded wait of the tensor-core GEMM runs out: ibfs_set_wait_limit's probe
+* a bounded wait of the tensor-core GEMM (the single-CTA kernel, or the
+  CTA-pair kernel) runs out: ibfs_set_wait_limit's probe
   makes every thread block wait on a barrier that nothing completes (2 ms
   limit) before it issues any copy or product; the advance returns
   IBFS_ERR_TIMEOUT naming that wait, each block frees its tensor memory, and a
@@ -54,12 +55,14 @@ def test_singular_force_system_is_chol_error():
     assert np.isfinite(ok.advance()["fx"]).all()
 
 
-@pytest.mark.parametrize("entry", ["advance", "advance_n"])
-def test_tensor_core_wait_limit_gives_timeout(entry):
+@pytest.mark.parametrize("entry,tile", [("advance", 0), ("advance_n", 0), ("advance", 4)])
+def test_tensor_core_wait_limit_gives_timeout(entry, tile):
+    """tile 4: every GEMM on the CTA-pair kernel, whose two CTAs meet at a
+    cluster barrier before freeing their tensor memory."""
     m, lev = 128, 3
     xb, yb = W.circle(4.0 / m)
     p = C.make_params(m, m, 0.004, 100.0, lev)
-    g = C.Solver(p, (xb, yb), C.make_options(precision=1))
+    g = C.Solver(p, (xb, yb), C.make_options(precision=1, tc_tile=tile))
     g.precompute()  # the factor is FP64 (no tensor-core GEMM); made before the probe is set
     g.set_wait_limit(0.002, probe=True)  # every GEMM block waits on a barrier nothing completes
     with pytest.raises(C.IbfsError) as e:
