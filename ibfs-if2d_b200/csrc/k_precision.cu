@@ -786,15 +786,15 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 
 // One 32 x 32 tile of one descriptor per block (block map entry {desc, tile},
 // tiles numbered i-fastest). The pass is bound by the bytes in flight, so each
-// block first issues its whole input as asynchronous 8-byte copies into
-// shared memory -- the source tile and, for a residual, x0 with a one-node
-// halo (zero outside the grid, which drops the stencil's boundary terms
-// exactly) -- and waits once. v is then assembled column-major (a warp reads
+// block first issues its whole input at once: each thread's four source values
+// as plain loads into registers and, for a residual, x0 with a one-node halo
+// (zero outside the grid, which drops the stencil's boundary terms exactly) as
+// asynchronous 8-byte copies into shared memory; then it waits once. v is then assembled column-major (a warp reads
 // 32 consecutive i) in place and written row-major as three BF16 slices, four
 // consecutive j per thread (8-byte stores; a warp writes four 64-byte row
 // segments per slice).
-__global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__ descs,
-                                                    const int2* __restrict__ bmap) {
+__global__ void __launch_bounds__(256, 8) k_prep_split(const PrepDesc* __restrict__ descs,
+                                                       const int2* __restrict__ bmap) {
   const int2 bm = bmap[blockIdx.x];
   const PrepDesc& d = descs[bm.x];
   const int M = d.m - 1, N = d.n - 1;
@@ -803,10 +803,16 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
   __shared__ double t[32][33];
   __shared__ double h[34][35];  // x0(i0 - 1 + a, j0 - 1 + b) at [b][a]
   const double* x0 = d.x0;
-  for (int e = threadIdx.x; e < 32 * 32; e += 256) {
-    const int a = e & 31, b = e >> 5, i = i0 + a, j = j0 + b;
-    if (i < M && j < N) cp_async8(&t[b][a], d.src + i + (size_t)j * M);
-    else t[b][a] = 0.0;
+  // each thread walks four consecutive rows of one column; its four source
+  // values (read by no other thread) go straight to registers, in flight
+  // together with the halo copies
+  const int tx = threadIdx.x & 31, lb0 = 4 * (threadIdx.x >> 5);
+  const int ic = i0 + tx;
+  double sv[4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int j = j0 + lb0 + r;
+    sv[r] = (ic < M && j < N) ? __ldg(d.src + ic + (size_t)j * M) : 0.0;
   }
   if (x0) {
     for (int e = threadIdx.x; e < 34 * 34; e += 256) {
@@ -818,17 +824,15 @@ __global__ void __launch_bounds__(256) k_prep_split(const PrepDesc* __restrict__
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  // each thread walks four consecutive rows of one column, keeping the x0
-  // column values the next row shares in registers
-  const int tx = threadIdx.x & 31, lb0 = 4 * (threadIdx.x >> 5);
-  const int ic = i0 + tx;
+  // the x0 column values the next row shares stay in registers
   double dn = x0 ? h[lb0][tx + 1] : 0.0, c = x0 ? h[lb0 + 1][tx + 1] : 0.0;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const int jj = lb0 + r, j = j0 + jj;
     const double up = x0 ? h[jj + 2][tx + 1] : 0.0;
+    t[jj][tx] = 0.0;  // the K padding of the slices reads zero
     if (ic < M && j < N) {
-      double v = d.src_scale * t[jj][tx];
+      double v = d.src_scale * sv[r];
       if (d.bcsrc) {
         const int a = ic + 1, b = j + 1;
         if (a == 1 || a == M || b == 1 || b == N)

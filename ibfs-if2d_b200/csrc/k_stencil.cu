@@ -148,7 +148,8 @@ __global__ void __launch_bounds__(256) k_rhs(const DevCase* __restrict__ cases, 
 // in flight: each block first issues its whole input as asynchronous 8-byte
 // copies into shared memory (omega with a one-node halo, the u and v faces
 // the flux averages read, rhs_old), waits once, and then computes from shared
-// memory. Four resident blocks per SM (at most 64 registers a thread).
+// memory (rhs_old, which each thread alone reads, straight into registers).
+// Four resident blocks per SM (at most 64 registers a thread).
 __device__ __forceinline__ double lap5_nodes(const double* __restrict__ x, int i, int j, int M, int N) {
   double c = x[i + (size_t)j * M];
   double s = 4.0 * c;
@@ -198,7 +199,7 @@ struct RhsTile {
   double om[34][35];  // omega(i0 - 1 + a, j0 - 1 + b) at [b][a] (node coordinates, 0-based)
   double u[33][35];   // u face (i0 + a, j0 + b) at [b][a], a < 34 (face coordinates, 0-based)
   double v[34][34];   // v face (i0 + a, j0 + b) at [b][a], a < 33
-  double t[32][33];   // rhs_old, then the assembled b
+  double t[32][33];   // the assembled b, [column][row]
 };
 
 __global__ void __launch_bounds__(256, 4) k_rhs_split(const DevCase* __restrict__ cases,
@@ -237,7 +238,15 @@ __global__ void __launch_bounds__(256, 4) k_rhs_split(const DevCase* __restrict_
     stage_window<35>(&S.om[0][0], om, M, M, N, i0 - 1, j0 - 1, 34, 34);
     stage_window<35>(&S.u[0][0], q, m + 1, m + 1, n, i0, j0, 34, 33);
     stage_window<34>(&S.v[0][0], qv, m, m, n + 1, i0, j0, 33, 34);
-    if (!euler) stage_window<33>(&S.t[0][0], ro, M, M, N, i0, j0, 32, 32);
+    // rhs_old of the thread's four nodes (read by no other thread): plain
+    // loads into registers, in flight together with the tile copies
+    const int la0 = tx, lr0 = 4 * ty;
+    double ro4[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int ia = i0 + la0, jb = j0 + lr0 + r;
+      ro4[r] = (!euler && ia < M && jb < N) ? ro[ia + (size_t)jb * M] : 0.0;
+    }
     cp_async_all();
     __syncthreads();
     const double u0 = C.q0_u1 * (double)(1 << (k - 1));
@@ -284,7 +293,7 @@ __global__ void __launch_bounds__(256, 4) k_rhs_split(const DevCase* __restrict_
         const double fqv_im = -0.5 * (ua_c * c + ua_m * WiL);
         const double rhs = fqv_i - fqv_im - fq_hi + fq_lo;
         fq_lo = fq_hi;
-        const double rold = euler ? rhs : S.t[lb][la];
+        const double rold = euler ? rhs : ro4[r];
         const int a = i - 1, b = j - 1;
         double rb = 0.0;
         if (a == 1 || a == m - 1 || b == 1 || b == n - 1) {
