@@ -67,6 +67,21 @@ def test_options_group_and_geometry(tmp_path):
     assert (p["istop"], p["isave"], p["dt"], p["re"], p["mgridlev"]) == (400, 25, 0.005, 300.0, 4)
 
 
+@pytest.mark.parametrize("tile,ok", [(0, True), (3, True), (4, True), (5, False), (-1, False)])
+def test_tensor_core_tile_option(tmp_path, tile, ok):
+    """TC_TILE picks the tensor-core GEMM's tile configuration: 0 (the
+    autotuner), 1..3 single-CTA tiles, 4 the CTA-pair tile; anything else is
+    refused before any CUDA call."""
+    write_inp(tmp_path, "&read_parameters m=32, n=32, len=4.0, offsetx=2.0, offsety=2.0 /\n"
+                        f"&B200_OPTIONS PRECISION=1, TC_TILE={tile} /\n")
+    rc, out, err = run(tmp_path)
+    if ok:
+        assert rc == 0, err
+        assert json.loads(out)["tc_tile"] == tile
+    else:
+        assert rc != 0 and "TC_TILE" in err
+
+
 def test_restart_record(tmp_path):
     m = n = 32
     L = 3
