@@ -18,9 +18,13 @@ def rel(a, b):
     return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
 
 
-@pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 1e-8)])
-def test_batch_vs_oracle(precision, tol):
+@pytest.mark.parametrize("precision,tol,tile", [(0, 1e-10, 0), (1, 1e-8, 0), (1, 1e-8, 4)])
+def test_batch_vs_oracle(precision, tol, tile):
+    """tile 4: every tensor-core GEMM of the split form on the CTA-pair tile,
+    the 32 x 24 case included."""
     params, bodies, opts = W.solver_args(SMALL, C, precision)
+    for o in opts:
+        o.tc_tile = tile
     g = C.Solver(params, bodies, opts)
     steps = 6
     hist = g.advance_n(steps)

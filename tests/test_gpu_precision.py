@@ -18,11 +18,13 @@ def rel(a, b):
     return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
 
 
-@pytest.mark.parametrize("m,n", [(64, 64), (128, 96), (200, 200)])
-def test_refined_solves(m, n):
+@pytest.mark.parametrize("m,n,tile", [(64, 64, 0), (128, 96, 0), (200, 200, 0), (128, 96, 4), (192, 384, 4)])
+def test_refined_solves(m, n, tile):
+    """ctci and ainv of the split form against the oracle, square and
+    rectangular grids; tile 4 puts every GEMM on the CTA-pair tile."""
     xb, yb = O.circle(4.0 / m, 1.0, 0.0, 0.0)
     oc = O.Case(O.make_params(m, n, 0.004, 100.0, 3), xb, yb)
-    g = C.Solver(C.make_params(m, n, 0.004, 100.0, 3), (xb, yb), C.make_options(precision=1))
+    g = C.Solver(C.make_params(m, n, 0.004, 100.0, 3), (xb, yb), C.make_options(precision=1, tc_tile=tile))
     x = np.random.default_rng(5).standard_normal(oc.ns)
     assert rel(g.apply_op(1, x), oc.ctci(x)) < 1e-9
     assert rel(g.apply_op(2, x), oc.ainv(x)) < 1e-9
