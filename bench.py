@@ -195,7 +195,9 @@ def issued_tensor_flops(cases, nlev):
     refinement): every solve is 4 GEMMs of 6 products (first pass) plus 4 of
     the correction's products -- 6 for the 2L Poisson solves of the two
     vort2flux calls, 3 for the L Crank-Nicolson solves and ainv -- on
-    128-row and 128-column padded tiles with K padded to 64."""
+    128-row and 128-column padded tiles with K padded to 64 (the single-CTA
+    tiles; a launch group on the 256 x 256 CTA-pair tile pads some grids
+    further, so this is a lower bound there)."""
     rup = lambda x, a: (x + a - 1) // a * a
     tot = 0.0
     for c, L in zip(cases, nlev):
